@@ -1,0 +1,163 @@
+/*
+ * sdtfe_b200.h - device-resident DTFE meshes on NVIDIA B200 (sm_100a).
+ *
+ * The drop-in entry points of the reference (dtfe.h, triangulate.h, utils.h,
+ * bitmap.h in this directory) are implemented on top of this handle API.  A
+ * handle owns one Delaunay mesh in GPU memory: vertex positions and DTFE
+ * densities, tet vertex/neighbour rows, per-tet gradients, the packed walk
+ * records of each precision and the projected forward hull per projection
+ * axis.  Every call returns a status; dtfe_last_error() gives the message of
+ * the calling thread's last failure.
+ *
+ * Host pointers are plain C arrays in the reference layouts:
+ *   particle_data  double[n*4]  (x, y, z, column 3 = density or field)
+ *   tetra_data     int[nt*8]    (A, B, C, D, n_BDC, n_ACD, n_ADB, n_ABC)
+ * Device pointers (the *_device calls) are CUDA global memory; a stream
+ * argument of NULL means the handle's own stream.
+ */
+#ifndef SDTFE_B200_H
+#define SDTFE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DTFE_OK = 0,
+  DTFE_ERR_INVALID = 1,       /* bad argument                                   */
+  DTFE_ERR_CUDA = 2,          /* CUDA runtime error                             */
+  DTFE_ERR_NOMEM = 3,         /* device allocation failed                       */
+  DTFE_ERR_MESH = 4,          /* index out of range in tetra_data               */
+  DTFE_ERR_UNSUPPORTED = 5,   /* argument outside what this build implements   */
+  DTFE_ERR_NO_TRIANGULATOR = 6, /* triangulate() called with no backend set     */
+  DTFE_ERR_ADMISSION = 7      /* request exceeds the serving memory budget      */
+} dtfe_status_t;
+
+/* arithmetic of the ray walk */
+typedef enum {
+  DTFE_FP64 = 0,  /* the reference's FP64 arithmetic, operation for operation */
+  DTFE_MIXED = 1  /* FP32 walk, FP64 only where a filter says FP32 may be wrong */
+} dtfe_precision_t;
+
+/* projection axis; x and y project along a cyclic permutation of (x, y, z) */
+typedef enum { DTFE_AXIS_Z = 0, DTFE_AXIS_X = 1, DTFE_AXIS_Y = 2 } dtfe_axis_t;
+
+/* per-ray outcome (the reference prints a warning and drops the sample) */
+typedef enum {
+  DTFE_RAY_OK = 0,
+  DTFE_RAY_MISS = 1,         /* outside the projected hull (src/dtfe.c:626)          */
+  DTFE_RAY_NO_EXIT = 2,      /* no enter/leave face pair (src/dtfe.c:321-325,344-348) */
+  DTFE_RAY_PERTURB_MAX = 3,  /* > PERTURB_MAX perturbations (src/dtfe.c:338-342)      */
+  DTFE_RAY_BUDGET = 4,       /* visit budget exhausted (corrupt neighbour links)      */
+  DTFE_RAY_LOC_BUDGET = 5    /* point location exceeded its step budget              */
+} dtfe_ray_status_t;
+
+#define DTFE_N_RAY_STATUS 6
+
+typedef struct dtfe_mesh_s *dtfe_mesh_t;
+
+/* Surface-density map: the arguments of compute_density (src/dtfe.h:27-29)
+ * plus the explicit sample seed and the walk controls. */
+typedef struct {
+  int grid_dim;          /* map side G; map[row*G + col]                         */
+  double box_len;        /* map width and height                                 */
+  double box_len_z;      /* slab depth along the projection axis                 */
+  double center[3];      /* in the original (x, y, z) frame                      */
+  int n_samples;         /* Monte Carlo samples per pixel (1..1024)               */
+  double delta_sample;   /* MC box width; the pixel width when smaller          */
+  uint64_t seed;         /* sample offsets sdtfe_sample_u01(seed, pixel, sample) */
+  int axis;              /* dtfe_axis_t                                          */
+  int precision;         /* dtfe_precision_t                                     */
+  int max_visits;        /* per-ray visit budget; <= 0 selects 2*n_tetra + 64     */
+} dtfe_map_params_t;
+
+typedef struct {
+  unsigned long long rays;
+  unsigned long long visits;                       /* tets crossed, summed over rays */
+  unsigned long long status[DTFE_N_RAY_STATUS];    /* rays per dtfe_ray_status_t     */
+  unsigned long long fp64_fallbacks;               /* MIXED: guarded FP64 re-tests   */
+  double walk_ms;                                  /* device time of the walk kernel */
+} dtfe_map_stats_t;
+
+typedef struct {
+  int n_particles;
+  int n_tetra;
+  int n_hull_tri[3];     /* forward-hull triangles per axis (-1: not built yet)  */
+  size_t device_bytes;   /* device memory held by the handle                     */
+  int fp32_exact;        /* 1 when every coordinate is exactly a float          */
+} dtfe_mesh_info_t;
+
+/* mesh flags */
+#define DTFE_MESH_FIELD 1u       /* column 3 is a field: skip the density step      */
+#define DTFE_MESH_NO_FP64_REC 2u /* keep no FP64 walk records (MIXED maps only)     */
+
+const char *dtfe_last_error(void);
+const char *dtfe_status_string(dtfe_status_t s);
+
+/* Upload a mesh and build everything the walks need.  Unless DTFE_MESH_FIELD is
+ * set, column 3 of particle_data is ignored and replaced on the device by the
+ * DTFE density 4*p_mass / (sum of adjacent |V|) (src/triangulate.c:183-225). */
+dtfe_status_t dtfe_mesh_create(const double *particle_data, int n_particles,
+                               const int *tetra_data, int n_tetra, float p_mass,
+                               unsigned flags, dtfe_mesh_t *out);
+dtfe_status_t dtfe_mesh_destroy(dtfe_mesh_t mesh);
+dtfe_status_t dtfe_mesh_info(dtfe_mesh_t mesh, dtfe_mesh_info_t *info);
+dtfe_status_t dtfe_mesh_sync(dtfe_mesh_t mesh);
+
+/* downloads (host pointers) */
+dtfe_status_t dtfe_mesh_density(dtfe_mesh_t mesh, double *rho /* n */);
+dtfe_status_t dtfe_mesh_gradients(dtfe_mesh_t mesh, double *grad /* 3*nt */);
+dtfe_status_t dtfe_mesh_adjacency(dtfe_mesh_t mesh, int *counts /* n */);
+dtfe_status_t dtfe_mesh_hull(dtfe_mesh_t mesh, int axis, int *tri /* 8*n_tri or NULL */,
+                             int *n_tri);
+
+/* Map into a host array (accumulated: map[p] += value, as the reference does). */
+dtfe_status_t dtfe_map(dtfe_mesh_t mesh, const dtfe_map_params_t *p, double *map,
+                       dtfe_map_stats_t *stats);
+/* Map into device memory, asynchronous on `stream` (accumulated as above). */
+dtfe_status_t dtfe_map_device(dtfe_mesh_t mesh, const dtfe_map_params_t *p, double *d_map,
+                              void *stream);
+/* Counters of the last map launched on this handle (synchronises). */
+dtfe_status_t dtfe_mesh_last_stats(dtfe_mesh_t mesh, dtfe_map_stats_t *stats);
+
+/* Rays at explicit positions (x[i], y[i]) in the projected frame of p->axis,
+ * walked over the slab z0 .. z0+lz; ray id i keys the perturbation stream.
+ * visits (optional) receives up to max_record tet indices per ray (-1 padded). */
+dtfe_status_t dtfe_trace(dtfe_mesh_t mesh, const dtfe_map_params_t *p, int n_rays,
+                         const double *x, const double *y, double z0, double lz,
+                         double delta_xy, double *rho, int *crossed, int *status,
+                         int *visits, int max_record);
+
+/* 3-D grid of interpolate_to_3d_grid (src/dtfe.c:668-735) into a host array of
+ * G^3 doubles, accumulated; grid[(i*G + j)*G + iz], i along x and j along y. */
+dtfe_status_t dtfe_grid(dtfe_mesh_t mesh, int grid_dim, double box_len, const double center[3],
+                        unsigned supersampling, uint64_t seed, double *grid);
+
+/* Defaults used by the drop-in entry points of dtfe.h. */
+void dtfe_set_default_precision(int precision);
+int dtfe_get_default_precision(void);
+/* Fix the sample seed of the drop-in entry points; 0 restores the default,
+ * which keys each call's samples with one value drawn from the C library's
+ * rand(), so that srand() keeps its meaning. */
+void dtfe_set_seed(uint64_t seed);
+
+/* Host Qhull backend for triangulate(): returns Qhull's Delaunay cells as
+ * simplices[nt*4] and neighbors[nt*4] (neighbour k opposite vertex k, -1 on
+ * the hull), malloc'd; returns 0 on success. */
+typedef int (*dtfe_triangulator_fn)(const double *xyz4, int n, const char *options,
+                                    int **simplices, int **neighbors, size_t *n_tetra,
+                                    void *user);
+void dtfe_set_triangulator(dtfe_triangulator_fn fn, void *user);
+/* The layout step of triangulate() (src/triangulate.c:63-175): Qhull cells to
+ * tetra_data rows, swapping B and C (and their neighbours) where
+ * (AB x AC) . AD > 0.  tetra_out holds nt*8 ints. */
+void dtfe_tetra_from_cells(const double *particle_data, const int *simplices,
+                           const int *neighbors, size_t n_tetra, int *tetra_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SDTFE_B200_H */

@@ -1,0 +1,531 @@
+// capi.cu - the C ABI: the dtfe_mesh_* handle API of sdtfe_b200.h and, on
+// top of it, the reference's dtfe.h / triangulate.h entry points.
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "dtfe.h"
+#include "mesh.h"
+#include "triangulate.h"
+
+struct dtfe_mesh_s {
+  sdtfe::Mesh m;
+  std::mutex mu;  // one call at a time per handle
+};
+
+namespace sdtfe {
+
+static thread_local char t_err[512] = "";
+
+dtfe_status_t set_error(dtfe_status_t s, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(t_err, sizeof(t_err), fmt, ap);
+  va_end(ap);
+  return s;
+}
+
+}  // namespace sdtfe
+
+using namespace sdtfe;
+
+namespace {
+
+int g_default_precision = -1;  // -1: read SDTFE_PRECISION once
+uint64_t g_seed = 0;
+dtfe_triangulator_fn g_tri_fn = nullptr;
+void* g_tri_user = nullptr;
+
+dtfe_status_t check_params(const Mesh& m, const dtfe_map_params_t* p) {
+  if (!p) return set_error(DTFE_ERR_INVALID, "params is NULL");
+  if (p->grid_dim < 1) return set_error(DTFE_ERR_INVALID, "grid_dim %d < 1", p->grid_dim);
+  if ((long long)p->grid_dim * p->grid_dim > (1LL << 31))
+    return set_error(DTFE_ERR_UNSUPPORTED, "grid_dim %d: more than 2^31 pixels", p->grid_dim);
+  if (p->n_samples < 1 || p->n_samples > 16384)
+    return set_error(DTFE_ERR_UNSUPPORTED, "n_samples %d not in 1..16384", p->n_samples);
+  if (!(p->box_len > 0) || !(p->box_len_z > 0))
+    return set_error(DTFE_ERR_INVALID, "box_len and box_len_z must be > 0");
+  if (p->axis < 0 || p->axis > 2) return set_error(DTFE_ERR_INVALID, "axis %d not in 0..2", p->axis);
+  if (p->precision != DTFE_FP64 && p->precision != DTFE_MIXED)
+    return set_error(DTFE_ERR_INVALID, "precision %d unknown", p->precision);
+  if (p->precision == DTFE_FP64 && (m.flags & DTFE_MESH_NO_FP64_REC))
+    return set_error(DTFE_ERR_INVALID, "FP64 map on a mesh built with DTFE_MESH_NO_FP64_REC");
+  if (!m.has_density) return set_error(DTFE_ERR_INVALID, "mesh has no density");
+  return DTFE_OK;
+}
+
+// records + hull for the map's axis and precision, on the mesh stream
+dtfe_status_t prepare_axis(Mesh& m, int axis, int precision) {
+  if (!m.grad) SDTFE_TRY(mesh_gradients(&m));
+  const bool want64 = precision == DTFE_FP64 || !(m.flags & DTFE_MESH_NO_FP64_REC);
+  const bool want32 = precision == DTFE_MIXED;
+  SDTFE_TRY(mesh_records(&m, axis, want64, want32 || m.rec32 != nullptr));
+  SDTFE_TRY(mesh_hull(&m, axis, nullptr, nullptr));
+  return DTFE_OK;
+}
+
+dtfe_status_t launch_map(Mesh& m, const dtfe_map_params_t* p, double* d_map, cudaStream_t s,
+                         double* rr = nullptr, int* rc = nullptr, int* rs = nullptr) {
+  const MapGeom g = map_geometry(m, *p);
+  if (p->precision == DTFE_MIXED) return launch_map32(m, g, d_map, s, rr, rc, rs);
+  return launch_map64(m, g, d_map, s, rr, rc, rs);
+}
+
+dtfe_status_t read_stats(Mesh& m, dtfe_map_stats_t* st) {
+  unsigned long long c[kStatCount];
+  SDTFE_CUDA(cudaMemcpy(c, m.stats, sizeof(c), cudaMemcpyDeviceToHost));
+  memset(st, 0, sizeof(*st));
+  st->rays = c[kStatRays];
+  st->visits = c[kStatVisits];
+  for (int k = 0; k < DTFE_N_RAY_STATUS; ++k) st->status[k] = c[kStatStatus0 + k];
+  st->fp64_fallbacks = c[kStatFallback];
+  float ms = 0.f;
+  if (m.timed) SDTFE_CUDA(cudaEventElapsedTime(&ms, m.ev0, m.ev1));
+  st->walk_ms = ms;
+  return DTFE_OK;
+}
+
+uint64_t call_seed() {
+  if (g_seed) return g_seed;
+  // one draw from the C library stream keys this call's samples
+  return ((uint64_t)(unsigned)rand() << 1) ^ 0x5bd1e995ULL;
+}
+
+void report(const char* fn) { fprintf(stderr, "sdtfe_b200: %s failed: %s\n", fn, dtfe_last_error()); }
+
+}  // namespace
+
+extern "C" {
+
+const char* dtfe_last_error(void) { return t_err; }
+
+const char* dtfe_status_string(dtfe_status_t s) {
+  switch (s) {
+    case DTFE_OK: return "ok";
+    case DTFE_ERR_INVALID: return "invalid argument";
+    case DTFE_ERR_CUDA: return "CUDA error";
+    case DTFE_ERR_NOMEM: return "out of device memory";
+    case DTFE_ERR_MESH: return "inconsistent mesh";
+    case DTFE_ERR_UNSUPPORTED: return "unsupported";
+    case DTFE_ERR_NO_TRIANGULATOR: return "no triangulator registered";
+    case DTFE_ERR_ADMISSION: return "admission refused";
+  }
+  return "unknown";
+}
+
+void dtfe_set_default_precision(int precision) { g_default_precision = precision; }
+
+int dtfe_get_default_precision(void) {
+  if (g_default_precision < 0) {
+    const char* e = getenv("SDTFE_PRECISION");
+    g_default_precision = (e && (!strcmp(e, "mixed") || !strcmp(e, "1"))) ? DTFE_MIXED : DTFE_FP64;
+  }
+  return g_default_precision;
+}
+
+void dtfe_set_seed(uint64_t seed) { g_seed = seed; }
+
+void dtfe_set_triangulator(dtfe_triangulator_fn fn, void* user) {
+  g_tri_fn = fn;
+  g_tri_user = user;
+}
+
+dtfe_status_t dtfe_mesh_create(const double* particle_data, int n_particles, const int* tetra_data,
+                               int n_tetra, float p_mass, unsigned flags, dtfe_mesh_t* out) {
+  if (!out) return set_error(DTFE_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  auto* h = new (std::nothrow) dtfe_mesh_s();
+  if (!h) return set_error(DTFE_ERR_NOMEM, "host allocation failed");
+  Mesh& m = h->m;
+  dtfe_status_t s = mesh_upload(&m, particle_data, n_particles, tetra_data, n_tetra, p_mass, flags);
+  if (s == DTFE_OK && !(flags & DTFE_MESH_FIELD)) s = mesh_density(&m);
+  if (s == DTFE_OK) s = mesh_gradients(&m);
+  if (s == DTFE_OK) {
+    const bool want64 = !(flags & DTFE_MESH_NO_FP64_REC);
+    s = mesh_records(&m, DTFE_AXIS_Z, want64, !want64);
+  }
+  if (s == DTFE_OK) s = mesh_hull(&m, DTFE_AXIS_Z, nullptr, nullptr);
+  if (s == DTFE_OK) {
+    cudaError_t e = cudaStreamSynchronize(m.stream);
+    if (e != cudaSuccess) s = set_error(DTFE_ERR_CUDA, "mesh build: %s", cudaGetErrorString(e));
+  }
+  if (s != DTFE_OK) {
+    mesh_free(&m);
+    delete h;
+    return s;
+  }
+  *out = h;
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_mesh_destroy(dtfe_mesh_t h) {
+  if (!h) return DTFE_OK;
+  mesh_free(&h->m);
+  delete h;
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_mesh_info(dtfe_mesh_t h, dtfe_mesh_info_t* info) {
+  if (!h || !info) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  info->n_particles = h->m.n;
+  info->n_tetra = h->m.nt;
+  for (int a = 0; a < 3; ++a) info->n_hull_tri[a] = h->m.ax[a].hull_built ? h->m.ax[a].n_tri : -1;
+  info->device_bytes = h->m.bytes;
+  info->fp32_exact = h->m.fp32_exact ? 1 : 0;
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_mesh_sync(dtfe_mesh_t h) {
+  if (!h) return set_error(DTFE_ERR_INVALID, "NULL mesh");
+  SDTFE_CUDA(cudaStreamSynchronize(h->m.stream));
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_mesh_density(dtfe_mesh_t h, double* rho) {
+  if (!h || (!rho && h->m.n)) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  if (!m.n) return DTFE_OK;
+  SDTFE_CUDA(cudaStreamSynchronize(m.stream));
+  SDTFE_CUDA(cudaMemcpy2D(rho, sizeof(double), reinterpret_cast<const char*>(m.pos) + 3 * sizeof(double),
+                          sizeof(double4), sizeof(double), m.n, cudaMemcpyDeviceToHost));
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_mesh_gradients(dtfe_mesh_t h, double* grad) {
+  if (!h || (!grad && h->m.nt)) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  if (!m.grad) SDTFE_TRY(mesh_gradients(&m));
+  SDTFE_CUDA(cudaStreamSynchronize(m.stream));
+  if (m.nt) SDTFE_CUDA(cudaMemcpy(grad, m.grad, sizeof(double) * 3 * (size_t)m.nt, cudaMemcpyDeviceToHost));
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_mesh_adjacency(dtfe_mesh_t h, int* counts) {
+  if (!h || (!counts && h->m.n)) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  if (!h->m.adj) return set_error(DTFE_ERR_INVALID, "mesh built with DTFE_MESH_FIELD has no adjacency counts");
+  SDTFE_CUDA(cudaStreamSynchronize(h->m.stream));
+  if (h->m.n) SDTFE_CUDA(cudaMemcpy(counts, h->m.adj, sizeof(int) * h->m.n, cudaMemcpyDeviceToHost));
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_mesh_hull(dtfe_mesh_t h, int axis, int* tri, int* n_tri) {
+  if (!h || !n_tri) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  if (axis < 0 || axis > 2) return set_error(DTFE_ERR_INVALID, "axis %d not in 0..2", axis);
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  SDTFE_TRY(mesh_hull(&m, axis, nullptr, nullptr));
+  SDTFE_CUDA(cudaStreamSynchronize(m.stream));
+  *n_tri = m.ax[axis].n_tri;
+  if (tri && m.ax[axis].n_tri)
+    SDTFE_CUDA(cudaMemcpy(tri, m.ax[axis].tri_rows, sizeof(int) * 8 * (size_t)m.ax[axis].n_tri,
+                          cudaMemcpyDeviceToHost));
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_map_device(dtfe_mesh_t h, const dtfe_map_params_t* p, double* d_map,
+                              void* stream) {
+  if (!h || !d_map) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  SDTFE_TRY(check_params(m, p));
+  const bool ready = m.rec_axis == p->axis && m.ax[p->axis].hull_built &&
+                     (p->precision == DTFE_FP64 ? m.rec64 != nullptr : m.rec32 != nullptr);
+  cudaStream_t s = stream ? (cudaStream_t)stream : m.stream;
+  if (!ready) {
+    SDTFE_TRY(prepare_axis(m, p->axis, p->precision));
+    if (s != m.stream) SDTFE_CUDA(cudaStreamSynchronize(m.stream));
+  }
+  return launch_map(m, p, d_map, s);
+}
+
+dtfe_status_t dtfe_mesh_last_stats(dtfe_mesh_t h, dtfe_map_stats_t* st) {
+  if (!h || !st) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  SDTFE_CUDA(cudaDeviceSynchronize());
+  return read_stats(h->m, st);
+}
+
+dtfe_status_t dtfe_map(dtfe_mesh_t h, const dtfe_map_params_t* p, double* map,
+                       dtfe_map_stats_t* stats) {
+  if (!h || !map) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  SDTFE_TRY(check_params(m, p));
+  SDTFE_TRY(prepare_axis(m, p->axis, p->precision));
+  cudaStream_t s = m.stream;
+  const size_t bytes = sizeof(double) * (size_t)p->grid_dim * p->grid_dim;
+  double* d_map = nullptr;
+  SDTFE_CUDA(cudaMallocAsync(&d_map, bytes, s));
+  SDTFE_CUDA(cudaMemcpyAsync(d_map, map, bytes, cudaMemcpyHostToDevice, s));
+  dtfe_status_t st = launch_map(m, p, d_map, s);
+  if (st == DTFE_OK) {
+    cudaError_t e = cudaMemcpyAsync(map, d_map, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "map: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(d_map, s);
+  if (st == DTFE_OK && stats) st = read_stats(m, stats);
+  return st;
+}
+
+dtfe_status_t dtfe_trace(dtfe_mesh_t h, const dtfe_map_params_t* p, int n_rays, const double* x,
+                         const double* y, double z0, double lz, double delta_xy, double* rho,
+                         int* crossed, int* status, int* visits, int max_record) {
+  if (!h || !p || n_rays < 0 || (n_rays && (!x || !y || !rho || !crossed || !status)))
+    return set_error(DTFE_ERR_INVALID, "NULL argument");
+  if (visits && max_record < 1) return set_error(DTFE_ERR_INVALID, "max_record < 1");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  if (p->axis < 0 || p->axis > 2) return set_error(DTFE_ERR_INVALID, "axis %d not in 0..2", p->axis);
+  SDTFE_TRY(prepare_axis(m, p->axis, p->precision));
+  if (!n_rays) return DTFE_OK;
+  cudaStream_t s = m.stream;
+  const long long mv = p->max_visits > 0 ? p->max_visits : 2LL * m.nt + 64;
+  const int max_visits = (int)(mv > 0x7fffffff ? 0x7fffffff : mv);
+  double *dx, *dy, *dr;
+  int *dc, *ds, *dv = nullptr;
+  SDTFE_CUDA(cudaMallocAsync(&dx, sizeof(double) * n_rays, s));
+  SDTFE_CUDA(cudaMallocAsync(&dy, sizeof(double) * n_rays, s));
+  SDTFE_CUDA(cudaMallocAsync(&dr, sizeof(double) * n_rays, s));
+  SDTFE_CUDA(cudaMallocAsync(&dc, sizeof(int) * n_rays, s));
+  SDTFE_CUDA(cudaMallocAsync(&ds, sizeof(int) * n_rays, s));
+  const size_t vbytes = visits ? sizeof(int) * (size_t)n_rays * max_record : 0;
+  if (visits) {
+    SDTFE_CUDA(cudaMallocAsync(&dv, vbytes, s));
+    SDTFE_CUDA(cudaMemsetAsync(dv, 0xff, vbytes, s));
+  }
+  SDTFE_CUDA(cudaMemcpyAsync(dx, x, sizeof(double) * n_rays, cudaMemcpyHostToDevice, s));
+  SDTFE_CUDA(cudaMemcpyAsync(dy, y, sizeof(double) * n_rays, cudaMemcpyHostToDevice, s));
+  dtfe_status_t st =
+      p->precision == DTFE_MIXED
+          ? launch_trace32(m, n_rays, dx, dy, z0, lz, delta_xy, p->seed, max_visits, dr, dc, ds, dv,
+                           max_record, s)
+          : launch_trace64(m, n_rays, dx, dy, z0, lz, delta_xy, p->seed, max_visits, dr, dc, ds, dv,
+                           max_record, s);
+  if (st == DTFE_OK) {
+    cudaError_t e = cudaMemcpyAsync(rho, dr, sizeof(double) * n_rays, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(crossed, dc, sizeof(int) * n_rays, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(status, ds, sizeof(int) * n_rays, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && visits) e = cudaMemcpyAsync(visits, dv, vbytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "trace: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(dx, s);
+  cudaFreeAsync(dy, s);
+  cudaFreeAsync(dr, s);
+  cudaFreeAsync(dc, s);
+  cudaFreeAsync(ds, s);
+  if (dv) cudaFreeAsync(dv, s);
+  return st;
+}
+
+dtfe_status_t dtfe_grid(dtfe_mesh_t h, int G, double box_len, const double center[3],
+                        unsigned ss, uint64_t seed, double* grid) {
+  if (!h || !center || !grid) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  if (G < 1 || ss < 1) return set_error(DTFE_ERR_INVALID, "grid_dim and supersampling must be >= 1");
+  if (!(box_len > 0)) return set_error(DTFE_ERR_INVALID, "box_len must be > 0");
+  if ((double)G * G * G * sizeof(double) > 1e12)
+    return set_error(DTFE_ERR_UNSUPPORTED, "grid_dim %d: grid larger than 1 TB", G);
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  if (!m.has_density) return set_error(DTFE_ERR_INVALID, "mesh has no density");
+  SDTFE_TRY(prepare_axis(m, DTFE_AXIS_Z, DTFE_FP64));
+  cudaStream_t s = m.stream;
+  const size_t bytes = sizeof(double) * (size_t)G * G * G;
+  double* d = nullptr;
+  SDTFE_CUDA(cudaMallocAsync(&d, bytes, s));
+  SDTFE_CUDA(cudaMemcpyAsync(d, grid, bytes, cudaMemcpyHostToDevice, s));
+  const int max_visits = (int)((2LL * m.nt + 64) > 0x7fffffff ? 0x7fffffff : (2LL * m.nt + 64));
+  dtfe_status_t st = launch_grid64(m, G, box_len, center, ss, seed, max_visits, d, s);
+  if (st == DTFE_OK) {
+    cudaError_t e = cudaMemcpyAsync(grid, d, bytes, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "grid: %s", cudaGetErrorString(e));
+  }
+  cudaFreeAsync(d, s);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// Drop-ins for src/dtfe.h and src/triangulate.h.
+
+void compute_density(double* particle_data, int n_particles, int* tetra_data, int n_tetra,
+                     int grid_dim, double box_len, double box_len_z, double* rho, float p_mass,
+                     double center_x, double center_y, double center_z, const int n_mc_samp,
+                     const double delta_sample) {
+  dtfe_mesh_t h = nullptr;
+  if (dtfe_mesh_create(particle_data, n_particles, tetra_data, n_tetra, p_mass, 0, &h) != DTFE_OK)
+    return report("compute_density");
+  dtfe_map_params_t p;
+  memset(&p, 0, sizeof(p));
+  p.grid_dim = grid_dim;
+  p.box_len = box_len;
+  p.box_len_z = box_len_z;
+  p.center[0] = center_x;
+  p.center[1] = center_y;
+  p.center[2] = center_z;
+  p.n_samples = n_mc_samp;
+  p.delta_sample = delta_sample;
+  p.seed = call_seed();
+  p.axis = DTFE_AXIS_Z;
+  p.precision = dtfe_get_default_precision();
+  // column 3 of the caller's array receives the densities, as pre_compute_vol does
+  std::vector<double> dens(n_particles > 0 ? n_particles : 0);
+  dtfe_status_t s = n_particles ? dtfe_mesh_density(h, dens.data()) : DTFE_OK;
+  if (s == DTFE_OK)
+    for (int i = 0; i < n_particles; ++i) particle_data[4 * (size_t)i + 3] = dens[i];
+  if (s == DTFE_OK) s = dtfe_map(h, &p, rho, nullptr);
+  if (s != DTFE_OK) report("compute_density");
+  dtfe_mesh_destroy(h);
+}
+
+void interpolate_to_3d_grid(double* particle_data, int n_particles, int* tetra_data, int n_tetra,
+                            int grid_dim, double box_len, double* grid, double center_x,
+                            double center_y, double center_z, unsigned supersampling) {
+  dtfe_mesh_t h = nullptr;
+  if (dtfe_mesh_create(particle_data, n_particles, tetra_data, n_tetra, 0.f, DTFE_MESH_FIELD, &h) !=
+      DTFE_OK)
+    return report("interpolate_to_3d_grid");
+  const double c[3] = {center_x, center_y, center_z};
+  if (dtfe_grid(h, grid_dim, box_len, c, supersampling, call_seed(), grid) != DTFE_OK)
+    report("interpolate_to_3d_grid");
+  dtfe_mesh_destroy(h);
+}
+
+void compute_3d_density(double* particle_data, int n_particles, int* tetra_data, int n_tetra,
+                        int grid_dim, double box_len, double* rho, float p_mass, double center_x,
+                        double center_y, double center_z, unsigned supersampling) {
+  dtfe_mesh_t h = nullptr;
+  if (dtfe_mesh_create(particle_data, n_particles, tetra_data, n_tetra, p_mass, 0, &h) != DTFE_OK)
+    return report("compute_3d_density");
+  std::vector<double> dens(n_particles > 0 ? n_particles : 0);
+  dtfe_status_t s = n_particles ? dtfe_mesh_density(h, dens.data()) : DTFE_OK;
+  if (s == DTFE_OK)
+    for (int i = 0; i < n_particles; ++i) particle_data[4 * (size_t)i + 3] = dens[i];
+  const double c[3] = {center_x, center_y, center_z};
+  if (s == DTFE_OK) s = dtfe_grid(h, grid_dim, box_len, c, supersampling, call_seed(), rho);
+  if (s != DTFE_OK) report("compute_3d_density");
+  dtfe_mesh_destroy(h);
+}
+
+// Density only: upload, volumes, CSR, densities, download into column 3.
+void pre_compute_vol(double** particle_data, int n_particles, int* tetra_data, int n_tetra,
+                     float p_mass) {
+  if (!particle_data) return;
+  Mesh m;
+  dtfe_status_t s = mesh_upload(&m, *particle_data, n_particles, tetra_data, n_tetra, p_mass, 0);
+  if (s == DTFE_OK) s = mesh_density(&m);
+  if (s == DTFE_OK && n_particles) {
+    cudaError_t e = cudaMemcpy2DAsync(*particle_data + 3, sizeof(double4),
+                                      reinterpret_cast<const char*>(m.pos) + 3 * sizeof(double),
+                                      sizeof(double4), sizeof(double), n_particles,
+                                      cudaMemcpyDeviceToHost, m.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
+    if (e != cudaSuccess) s = set_error(DTFE_ERR_CUDA, "pre_compute_vol: %s", cudaGetErrorString(e));
+  }
+  if (s != DTFE_OK) report("pre_compute_vol");
+  mesh_free(&m);
+}
+
+// Gradients from the densities already in column 3 (the reference reads them
+// from particle_data the same way).
+double* gradients(int* tetra_data, int n_tetra, double* particle_data) {
+  double* out = (double*)malloc(sizeof(double) * 3 * (size_t)(n_tetra > 0 ? n_tetra : 1));
+  if (!out) return nullptr;
+  // the reference signature carries no particle count: use the largest vertex id
+  int n = 0;
+  for (int t = 0; t < n_tetra; ++t)
+    for (int k = 0; k < 4; ++k)
+      if (tetra_data[8 * (size_t)t + k] + 1 > n) n = tetra_data[8 * (size_t)t + k] + 1;
+  Mesh m;
+  dtfe_status_t s = mesh_upload(&m, particle_data, n, tetra_data, n_tetra, 0.f, DTFE_MESH_FIELD);
+  if (s == DTFE_OK) s = mesh_gradients(&m);
+  if (s == DTFE_OK && n_tetra) {
+    cudaError_t e = cudaMemcpyAsync(out, m.grad, sizeof(double) * 3 * (size_t)n_tetra,
+                                    cudaMemcpyDeviceToHost, m.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
+    if (e != cudaSuccess) s = set_error(DTFE_ERR_CUDA, "gradients: %s", cudaGetErrorString(e));
+  }
+  mesh_free(&m);
+  if (s != DTFE_OK) {
+    report("gradients");
+    free(out);
+    return nullptr;
+  }
+  return out;
+}
+
+int find_forward_hull(int* tetra_data, int n_tetra, double* particle_data, int n_particles,
+                      word_t* bitmap) {
+  Mesh m;
+  int count = 0;
+  std::vector<uint32_t> mask(n_tetra > 0 ? n_tetra : 0);
+  dtfe_status_t s = mesh_upload(&m, particle_data, n_particles, tetra_data, n_tetra, 0.f,
+                                DTFE_MESH_FIELD);
+  if (s == DTFE_OK) s = mesh_hull_mask(&m, DTFE_AXIS_Z, mask.data(), &count);
+  mesh_free(&m);
+  if (s != DTFE_OK) {
+    report("find_forward_hull");
+    return 0;
+  }
+  for (int t = 0; t < n_tetra; ++t) bitmap[t] |= mask[t] & 0xFu;  // word t holds tet t's faces
+  return count;
+}
+
+int* copy_fh_triangles(int* tetra_data, int n_tetra, double* particle_data, int n_particles,
+                       int n_tri, word_t* bitmap) {
+  int* out = (int*)malloc(sizeof(int) * 8 * (size_t)(n_tri > 0 ? n_tri : 1));
+  if (!out) return nullptr;
+  Mesh m;
+  int count = 0;
+  dtfe_status_t s = mesh_upload(&m, particle_data, n_particles, tetra_data, n_tetra, 0.f,
+                                DTFE_MESH_FIELD);
+  if (s == DTFE_OK) s = mesh_hull(&m, DTFE_AXIS_Z, bitmap, &count);
+  if (s == DTFE_OK && count != n_tri)
+    s = set_error(DTFE_ERR_INVALID, "bitmap holds %d faces, n_tri is %d", count, n_tri);
+  if (s == DTFE_OK && count) {
+    cudaError_t e = cudaMemcpyAsync(out, m.ax[0].tri_rows, sizeof(int) * 8 * (size_t)count,
+                                    cudaMemcpyDeviceToHost, m.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
+    if (e != cudaSuccess) s = set_error(DTFE_ERR_CUDA, "copy_fh_triangles: %s", cudaGetErrorString(e));
+  }
+  mesh_free(&m);
+  if (s != DTFE_OK) {
+    report("copy_fh_triangles");
+    free(out);
+    return nullptr;
+  }
+  return out;
+}
+
+int* triangulate(double* particle_data, int n_particles, size_t* num_facets, const char* options) {
+  if (num_facets) *num_facets = 0;
+  if (!g_tri_fn) {
+    set_error(DTFE_ERR_NO_TRIANGULATOR, "no Qhull backend registered (dtfe_set_triangulator)");
+    fprintf(stderr, "TRIANGULATION ERROR: %s\n", dtfe_last_error());
+    return nullptr;
+  }
+  int *simp = nullptr, *nb = nullptr;
+  size_t nt = 0;
+  if (g_tri_fn(particle_data, n_particles, options, &simp, &nb, &nt, g_tri_user) != 0 || !simp || !nb) {
+    free(simp);
+    free(nb);
+    set_error(DTFE_ERR_MESH, "triangulator failed");
+    fprintf(stderr, "TRIANGULATION ERROR: %s\n", dtfe_last_error());
+    return nullptr;
+  }
+  int* tetra = (int*)malloc(sizeof(int) * 8 * (nt ? nt : 1));
+  if (tetra) dtfe_tetra_from_cells(particle_data, simp, nb, nt, tetra);
+  free(simp);
+  free(nb);
+  if (tetra && num_facets) *num_facets = nt;
+  return tetra;
+}
+
+}  // extern "C"

@@ -1,0 +1,119 @@
+// mesh.h - the device-resident mesh behind a dtfe_mesh_t handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "sdtfe_b200.h"
+#include "walk64.cuh"
+#include "walk32.cuh"
+
+namespace sdtfe {
+
+// thread-local last error (capi.cu)
+dtfe_status_t set_error(dtfe_status_t s, const char* fmt, ...);
+
+#define SDTFE_CUDA(expr)                                                                  \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return ::sdtfe::set_error(e_ == cudaErrorMemoryAllocation ? DTFE_ERR_NOMEM           \
+                                                                : DTFE_ERR_CUDA,          \
+                                "%s:%d %s: %s", __FILE__, __LINE__, #expr,                 \
+                                cudaGetErrorString(e_));                                  \
+  } while (0)
+
+#define SDTFE_TRY(expr)                 \
+  do {                                  \
+    dtfe_status_t s_ = (expr);          \
+    if (s_ != DTFE_OK) return s_;       \
+  } while (0)
+
+// Counters of one map launch, in device memory.
+enum StatSlot : int {
+  kStatRays = 0,
+  kStatVisits = 1,
+  kStatStatus0 = 2,  // .. kStatStatus0 + DTFE_N_RAY_STATUS - 1
+  kStatFallback = kStatStatus0 + DTFE_N_RAY_STATUS,
+  kStatCount
+};
+
+struct AxisData {
+  bool hull_built = false;
+  int n_tri = 0;
+  TriRec64* tri = nullptr;  // device, n_tri records
+  int* tri_rows = nullptr;  // device, n_tri * 8 ints in the reference's tri_data layout
+};
+
+struct Mesh {
+  int n = 0, nt = 0;
+  float p_mass = 0.f;
+  unsigned flags = 0;
+  bool fp32_exact = false;
+  bool has_density = false;
+  cudaStream_t stream = nullptr;
+  double4* pos = nullptr;   // (x, y, z, rho) in the original frame
+  int4* rows = nullptr;     // 2 per tet: vertex ids, neighbour ids
+  double* grad = nullptr;   // 3 per tet
+  int* adj = nullptr;       // tets incident to each vertex
+  int rec_axis = -1;        // axis the walk records are built for
+  TetRec64* rec64 = nullptr;
+  TetRec32* rec32 = nullptr;
+  AxisData ax[3];
+  unsigned long long* stats = nullptr;  // kStatCount counters of the last map
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timed = false;       // ev0/ev1 bracket the last walk launch
+  size_t bytes = 0;
+};
+
+// mesh.cu
+dtfe_status_t mesh_upload(Mesh* m, const double* particle_data, int n, const int* tetra_data,
+                          int nt, float p_mass, unsigned flags);
+dtfe_status_t mesh_density(Mesh* m);
+dtfe_status_t mesh_gradients(Mesh* m);
+dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32);
+// host_mask (optional) replaces the forward-face test with a caller's bitmap
+// (one 32-bit word per tet, faces in bits 0..3)
+dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count_out);
+dtfe_status_t mesh_hull_mask(Mesh* m, int axis, uint32_t* host_mask_out, int* count_out);
+void mesh_free(Mesh* m);
+
+// Cyclic permutation of the projection axis: the walk sees (x', y', z').
+__host__ __device__ inline void permute3(int axis, double x, double y, double z, double* px,
+                                         double* py, double* pz) {
+  if (axis == 1) {  // along x: (y, z, x)
+    *px = y; *py = z; *pz = x;
+  } else if (axis == 2) {  // along y: (z, x, y)
+    *px = z; *py = x; *pz = y;
+  } else {
+    *px = x; *py = y; *pz = z;
+  }
+}
+
+// walk.cu / walk32.cu launchers
+struct MapGeom {
+  int G, S;
+  double dxy, offx, offy, offz, lz, scale, soff, dist;
+  uint64_t seed;
+  int max_visits;
+};
+MapGeom map_geometry(const Mesh& m, const dtfe_map_params_t& p);
+dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
+                           double* ray_rho, int* ray_crossed, int* ray_status);
+dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
+                           double* ray_rho, int* ray_crossed, int* ray_status);
+dtfe_status_t launch_trace64(Mesh& m, int n_rays, const double* d_x, const double* d_y, double z0,
+                             double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
+                             int* d_crossed, int* d_status, int* d_visits, int max_record,
+                             cudaStream_t s);
+dtfe_status_t launch_trace32(Mesh& m, int n_rays, const double* d_x, const double* d_y, double z0,
+                             double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
+                             int* d_crossed, int* d_status, int* d_visits, int max_record,
+                             cudaStream_t s);
+dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
+                            uint64_t seed, int max_visits, double* d_grid, cudaStream_t s);
+
+}  // namespace sdtfe

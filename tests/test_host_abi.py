@@ -1,0 +1,193 @@
+"""CPU-side checks of the C-ABI library: it loads, exports every function the
+headers in include/ declare, and its host-side routines (input preparation,
+face bitmap, the layout step of triangulate) match the reference bit for bit.
+Nothing here launches a kernel."""
+import ctypes
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_set
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        if os.path.basename(h) == "sdtfe_rng.h":  # header-only inline functions
+            continue
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"//[^\n]*", "", src)
+        src = re.sub(r"#[^\n]*", "", src)
+        src = src.replace('extern "C" {', "").replace("}", "")
+        for stmt in src.split(";"):
+            stmt = " ".join(stmt.split())
+            if not stmt or stmt.startswith("typedef") or "{" in stmt:
+                continue
+            m = re.match(r"^(?:extern \"C\" )?[\w\s\*]*?\b(\w+)\s*\(", stmt)
+            if m and "static" not in stmt:
+                names.add(m.group(1))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_function():
+    from sdtfe_b200 import lib
+
+    L = lib()
+    names = declared_functions()
+    assert "compute_density" in names and "dtfe_mesh_create" in names and len(names) > 30
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_library_is_native_and_in_tree():
+    from sdtfe_b200 import _lib
+
+    assert os.path.dirname(_lib.LIB_PATH) == os.path.join(ROOT, "sdtfe_b200")
+    assert os.path.exists(_lib.LIB_PATH)
+
+
+def test_convert_rotate_shuffle_match_reference(golden):
+    from sdtfe_b200 import lib
+
+    L = lib()
+    g = golden_set(golden, "prep")
+    soa = np.ascontiguousarray(g["soa"])
+    q = L.convert_to_qhdata(soa, soa.shape[1])
+    arr = np.ctypeslib.as_array(ctypes.cast(q, ctypes.POINTER(ctypes.c_double)), shape=(200,)).copy()
+    ctypes.CDLL(None).free(ctypes.c_void_p(q))
+    arr = arr.reshape(50, 4)
+    assert np.array_equal(arr, g["qhdata"])
+    rot = arr.copy()
+    L.rotate3d(rot, 50, np.array([0.3, 1.1, -2.0]), np.array([0.5, 0.4, 0.6]))
+    assert np.array_equal(rot, g["rotated"])
+    libc = ctypes.CDLL(None)
+    libc.srand(12345)
+    shuf = arr.copy()
+    L.shuffle_buff(shuf, 50, 20)
+    assert np.array_equal(shuf, g["shuffled"])
+
+
+def test_bitmap_layout():
+    from sdtfe_b200 import lib
+
+    L = lib()
+    L.set_bit.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.get_bit.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.clear_bit.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.delete_bitmap.argtypes = [ctypes.c_void_p]
+    n_tet = 10
+    bm = L.create_bitmap(n_tet * 4)
+    words = np.ctypeslib.as_array(ctypes.cast(bm, ctypes.POINTER(ctypes.c_uint32)), shape=(n_tet + 1,))
+    assert not words.any()
+    L.set_bit(bm, 4 * 7 + 2)  # face 2 of tet 7
+    L.set_bit(bm, 4 * 3 + 0)
+    assert words[7] == 1 << 2 and words[3] == 1
+    assert L.get_bit(bm, 30) == 1 and L.get_bit(bm, 31) == 0
+    L.clear_bit(bm, 30)
+    assert words[7] == 0
+    L.delete_bitmap(bm)
+
+
+def test_tetra_layout_matches_numpy_restatement():
+    from scipy.spatial import Delaunay
+
+    from oracle.oracle import qhull_to_tetra, to_pos4
+    from sdtfe_b200 import tetra_from_cells
+
+    rng = np.random.default_rng(5)
+    pos4 = to_pos4(rng.random((2000, 3)))
+    d = Delaunay(pos4[:, :3], qhull_options="Qt Qbb Qz")
+    a = tetra_from_cells(pos4, d.simplices, d.neighbors)
+    b = qhull_to_tetra(pos4, d.simplices, d.neighbors)
+    assert np.array_equal(a, b)
+    # every tet ends with (AB x AC) . AD <= 0 (src/triangulate.c:92-100)
+    p = pos4[:, :3]
+    A, B, C, D = (p[a[:, k]] for k in range(4))
+    assert (np.einsum("ij,ij->i", np.cross(B - A, C - A), D - A) <= 0).all()
+
+
+def test_triangulate_without_backend_returns_null(capfd):
+    from sdtfe_b200 import lib
+
+    L = lib()
+    L.triangulate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
+                              ctypes.c_char_p]
+    L.triangulate.restype = ctypes.c_void_p
+    L.dtfe_set_triangulator(None, None)
+    pos = np.zeros((8, 4))
+    nf = ctypes.c_size_t(7)
+    assert L.triangulate(pos.ctypes.data, 8, ctypes.byref(nf), b"qhull d Qz Qt Qbb") is None
+    assert nf.value == 0
+    assert "TRIANGULATION ERROR" in capfd.readouterr().err
+
+
+def test_triangulate_with_registered_backend():
+    """triangulate() calls the registered host Qhull and lays out its cells."""
+    from scipy.spatial import Delaunay
+
+    from oracle.oracle import qhull_to_tetra, to_pos4
+    from sdtfe_b200 import lib
+
+    L = lib()
+    libc = ctypes.CDLL(None)
+    libc.malloc.restype = ctypes.c_void_p
+    libc.malloc.argtypes = [ctypes.c_size_t]
+    L.triangulate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
+                              ctypes.c_char_p]
+    L.triangulate.restype = ctypes.c_void_p
+    FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p,
+                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                          ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p)
+    seen = {}
+
+    def backend(xyz4, n, options, simp, nbr, nt, user):
+        pts = np.ctypeslib.as_array(ctypes.cast(xyz4, ctypes.POINTER(ctypes.c_double)),
+                                    shape=(n, 4))[:, :3].copy()
+        seen["options"] = options
+        d = Delaunay(pts, qhull_options="Qt Qbb Qz")
+        for arr, out in ((d.simplices, simp), (d.neighbors, nbr)):
+            a = np.ascontiguousarray(arr, np.int32)
+            p = libc.malloc(a.nbytes)
+            ctypes.memmove(p, a.ctypes.data, a.nbytes)
+            out[0] = p
+        nt[0] = len(d.simplices)
+        return 0
+
+    cb = FN(backend)
+    L.dtfe_set_triangulator.argtypes = [FN, ctypes.c_void_p]
+    L.dtfe_set_triangulator(cb, None)
+    try:
+        rng = np.random.default_rng(8)
+        pos4 = to_pos4(rng.random((300, 3)))
+        nf = ctypes.c_size_t(0)
+        ptr = L.triangulate(pos4.ctypes.data, 300, ctypes.byref(nf), b"qhull d Qz Qt Qbb")
+        assert ptr and nf.value > 0
+        got = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_int)),
+                                    shape=(nf.value, 8)).copy()
+        libc.free.argtypes = [ctypes.c_void_p]
+        libc.free(ptr)
+        d = Delaunay(pos4[:, :3], qhull_options="Qt Qbb Qz")
+        assert np.array_equal(got, qhull_to_tetra(pos4, d.simplices, d.neighbors))
+        assert seen["options"] == b"qhull d Qz Qt Qbb"
+    finally:
+        L.dtfe_set_triangulator.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.dtfe_set_triangulator(None, None)
+
+
+def test_mesh_create_reports_cuda_failure_without_gpu():
+    """On a machine without a usable GPU the handle API returns an error status
+    (and never runs anything on the CPU instead)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from oracle.oracle import to_pos4
+    from sdtfe_b200 import DTFEError, Mesh
+
+    pos4 = to_pos4(np.random.default_rng(0).random((10, 3)))
+    with pytest.raises(DTFEError):
+        Mesh(pos4, np.zeros((1, 8), np.int32))
