@@ -88,7 +88,17 @@ typedef struct {
   int n_hull_tri[3];     /* forward-hull triangles per axis (-1: not built yet)  */
   size_t device_bytes;   /* device memory held by the handle                     */
   int fp32_exact;        /* 1 when every coordinate is exactly a float          */
+  int map_variant;       /* mixed-map kernel variant in use (dtfe_autotune)      */
 } dtfe_mesh_info_t;
+
+/* One mixed-map kernel variant: threads per block, blocks per SM the register
+ * budget allows, and the pixel tile shape (0: square-ish, 1: row strip). */
+typedef struct {
+  int block;
+  int min_blocks;
+  int wide_tile;
+  double ms;             /* autotuner timing on its window (0 if not timed)     */
+} dtfe_variant_t;
 
 /* mesh flags */
 #define DTFE_MESH_FIELD 1u       /* column 3 is a field: skip the density step      */
@@ -136,6 +146,16 @@ dtfe_status_t dtfe_trace(dtfe_mesh_t mesh, const dtfe_map_params_t *p, int n_ray
 dtfe_status_t dtfe_grid(dtfe_mesh_t mesh, int grid_dim, double box_len, const double center[3],
                         unsigned supersampling, uint64_t seed, double *grid);
 
+/* Autotuner for the mixed-precision map kernel: times every variant on a
+ * central window of the map p describes (same pixel size and samples, about a
+ * sixteenth of the pixels), keeps the fastest for this handle and returns its
+ * index.  timings (optional) receives dtfe_num_variants() entries. */
+int dtfe_num_variants(void);
+dtfe_status_t dtfe_autotune(dtfe_mesh_t mesh, const dtfe_map_params_t *p, int *best,
+                            dtfe_variant_t *timings);
+/* Select a variant explicitly (-1: the built-in default). */
+dtfe_status_t dtfe_set_variant(dtfe_mesh_t mesh, int variant);
+
 /* Defaults used by the drop-in entry points of dtfe.h. */
 void dtfe_set_default_precision(int precision);
 int dtfe_get_default_precision(void);
@@ -143,6 +163,10 @@ int dtfe_get_default_precision(void);
  * which keys each call's samples with one value drawn from the C library's
  * rand(), so that srand() keeps its meaning. */
 void dtfe_set_seed(uint64_t seed);
+
+/* Number of CUDA kernels this library has launched in this process (all
+ * handles); benchmarks read it before and after a timed region. */
+unsigned long long dtfe_kernel_launches(void);
 
 /* Host Qhull backend for triangulate(): returns Qhull's Delaunay cells as
  * simplices[nt*4] and neighbors[nt*4] (neighbour k opposite vertex k, -1 on

@@ -62,7 +62,12 @@ class MeshInfo(ctypes.Structure):
         ("n_hull_tri", _i * 3),
         ("device_bytes", ctypes.c_size_t),
         ("fp32_exact", _i),
+        ("map_variant", _i),
     ]
+
+
+class Variant(ctypes.Structure):
+    _fields_ = [("block", _i), ("min_blocks", _i), ("wide_tile", _i), ("ms", _d)]
 
 
 class DTFEError(RuntimeError):
@@ -103,6 +108,9 @@ def lib() -> ctypes.CDLL:
     L.dtfe_grid.argtypes = [_vp, _i, _d, _d * 3, ctypes.c_uint, ctypes.c_uint64, _f64]
     L.dtfe_set_default_precision.argtypes = [_i]
     L.dtfe_set_seed.argtypes = [ctypes.c_uint64]
+    L.dtfe_kernel_launches.restype = ctypes.c_ulonglong
+    L.dtfe_autotune.argtypes = [_vp, ctypes.POINTER(MapParams), ctypes.POINTER(_i), _vp]
+    L.dtfe_set_variant.argtypes = [_vp, _i]
     L.dtfe_tetra_from_cells.argtypes = [_f64, _i32, _i32, ctypes.c_size_t, _i32]
     # drop-ins
     L.compute_density.argtypes = [_f64, _i, _i32, _i, _i, _d, _d, _f64, ctypes.c_float, _d, _d,
@@ -234,6 +242,19 @@ class Mesh:
     def map_device(self, params: MapParams, d_map_ptr: int, stream_ptr: int = 0):
         _check(lib().dtfe_map_device(self.h, ctypes.byref(params), _vp(d_map_ptr),
                                      _vp(stream_ptr) if stream_ptr else None))
+
+    def autotune(self, params: MapParams):
+        """Pick the fastest mixed-map kernel variant for maps like `params`.
+        Returns (best index, list of per-variant dicts)."""
+        n = lib().dtfe_num_variants()
+        arr = (Variant * n)()
+        best = _i()
+        _check(lib().dtfe_autotune(self.h, ctypes.byref(params), ctypes.byref(best), arr))
+        return best.value, [dict(block=v.block, min_blocks=v.min_blocks, wide_tile=v.wide_tile,
+                                 ms=v.ms) for v in arr]
+
+    def set_variant(self, variant: int):
+        _check(lib().dtfe_set_variant(self.h, variant))
 
     def last_stats(self) -> MapStats:
         st = MapStats()

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -28,6 +29,10 @@ dtfe_status_t set_error(dtfe_status_t s, const char* fmt, ...) {
   va_end(ap);
   return s;
 }
+
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 }  // namespace sdtfe
 
@@ -129,6 +134,8 @@ int dtfe_get_default_precision(void) {
 
 void dtfe_set_seed(uint64_t seed) { g_seed = seed; }
 
+unsigned long long dtfe_kernel_launches(void) { return g_launches.load(); }
+
 void dtfe_set_triangulator(dtfe_triangulator_fn fn, void* user) {
   g_tri_fn = fn;
   g_tri_user = user;
@@ -176,6 +183,7 @@ dtfe_status_t dtfe_mesh_info(dtfe_mesh_t h, dtfe_mesh_info_t* info) {
   for (int a = 0; a < 3; ++a) info->n_hull_tri[a] = h->m.ax[a].hull_built ? h->m.ax[a].n_tri : -1;
   info->device_bytes = h->m.bytes;
   info->fp32_exact = h->m.fp32_exact ? 1 : 0;
+  info->map_variant = h->m.tune32;
   return DTFE_OK;
 }
 
@@ -242,6 +250,64 @@ dtfe_status_t dtfe_map_device(dtfe_mesh_t h, const dtfe_map_params_t* p, double*
     if (s != m.stream) SDTFE_CUDA(cudaStreamSynchronize(m.stream));
   }
   return launch_map(m, p, d_map, s);
+}
+
+int dtfe_num_variants(void) { return num_map32_variants(); }
+
+dtfe_status_t dtfe_set_variant(dtfe_mesh_t h, int variant) {
+  if (!h) return set_error(DTFE_ERR_INVALID, "NULL mesh");
+  if (variant < -1 || variant >= num_map32_variants())
+    return set_error(DTFE_ERR_INVALID, "variant %d not in -1..%d", variant, num_map32_variants() - 1);
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->m.tune32 = variant;
+  return DTFE_OK;
+}
+
+dtfe_status_t dtfe_autotune(dtfe_mesh_t h, const dtfe_map_params_t* p, int* best,
+                            dtfe_variant_t* timings) {
+  if (!h || !p) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  SDTFE_TRY(check_params(m, p));
+  dtfe_map_params_t q = *p;
+  q.precision = DTFE_MIXED;
+  // central window: a quarter of the side, at the same pixel size
+  q.grid_dim = p->grid_dim >= 128 ? p->grid_dim / 4 : p->grid_dim;
+  q.box_len = p->box_len * q.grid_dim / p->grid_dim;
+  SDTFE_TRY(prepare_axis(m, q.axis, q.precision));
+  cudaStream_t s = m.stream;
+  double* d_map = nullptr;
+  const size_t bytes = sizeof(double) * (size_t)q.grid_dim * q.grid_dim;
+  SDTFE_CUDA(cudaMallocAsync(&d_map, bytes, s));
+  const int nv = num_map32_variants();
+  int best_v = -1;
+  float best_ms = 0.f;
+  dtfe_status_t st = DTFE_OK;
+  for (int v = 0; v < nv && st == DTFE_OK; ++v) {
+    m.tune32 = v;
+    float ms_v = 0.f;
+    for (int rep = 0; rep < 3 && st == DTFE_OK; ++rep) {  // first run warms the caches
+      st = launch_map(m, &q, d_map, s);
+      if (st != DTFE_OK) break;
+      cudaError_t e = cudaEventSynchronize(m.ev1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, m.ev0, m.ev1);
+      if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+      if (rep == 1 || (rep == 2 && ms < ms_v)) ms_v = ms;
+    }
+    if (timings) {
+      map32_variant_info(v, &timings[v].block, &timings[v].min_blocks, &timings[v].wide_tile);
+      timings[v].ms = ms_v;
+    }
+    if (st == DTFE_OK && (best_v < 0 || ms_v < best_ms)) {
+      best_v = v;
+      best_ms = ms_v;
+    }
+  }
+  cudaFreeAsync(d_map, s);
+  m.tune32 = best_v;
+  if (best) *best = best_v;
+  return st;
 }
 
 dtfe_status_t dtfe_mesh_last_stats(dtfe_mesh_t h, dtfe_map_stats_t* st) {

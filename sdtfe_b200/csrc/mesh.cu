@@ -37,13 +37,17 @@ __global__ void k_validate(const int4* __restrict__ rows, int nt, int n, int* __
   if (bad_v || bad_n(nb.x) || bad_n(nb.y) || bad_n(nb.z) || bad_n(nb.w)) atomicOr(err, 1);
 }
 
-// The four float-exactness flags of each coordinate.
-__global__ void k_fp32_exact(const double4* __restrict__ pos, int n, int* __restrict__ not_exact) {
+// Whether every coordinate is exactly a float, and the largest coordinate
+// magnitude (as float bits, rounded up; non-negative floats order as ints).
+__global__ void k_fp32_exact(const double4* __restrict__ pos, int n, int* __restrict__ not_exact,
+                             int* __restrict__ max_bits) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double4 p = pos[i];
   if ((double)(float)p.x != p.x || (double)(float)p.y != p.y || (double)(float)p.z != p.z)
     atomicOr(not_exact, 1);
+  const float mx = __double2float_ru(fmax(fabs(p.x), fmax(fabs(p.y), fabs(p.z))));
+  atomicMax(max_bits, __float_as_int(mx));
 }
 
 // a3 part 1: |det(A-D, B-D, C-D)|/6, the reference's expansion order
@@ -142,10 +146,9 @@ __global__ void k_gradients(const double4* __restrict__ pos, const int4* __restr
 }
 
 // Walk records for projection axis `axis`: positions and gradient permuted
-// cyclically, rho_A and the neighbour links copied.  The FP32 record also
-// flags tets whose FP32 field evaluation would lose more than a few ulps
-// (large gradient-to-value ratio across the tet: a sliver); the mixed walk
-// evaluates those from the FP64 record.
+// cyclically, the neighbour links copied.  The FP64 record carries rho_A and
+// the gradient (the reference's field form); the FP32 record carries the four
+// vertex densities (the mixed walk's barycentric form of the same field).
 __global__ void k_records(const double4* __restrict__ pos, const int4* __restrict__ rows,
                           const double* __restrict__ grad, int nt, int axis,
                           TetRec64* __restrict__ r64, TetRec32* __restrict__ r32) {
@@ -177,19 +180,9 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
     r.xyab = make_float4((float)q[0][0], (float)q[0][1], (float)q[1][0], (float)q[1][1]);
     r.xycd = make_float4((float)q[2][0], (float)q[2][1], (float)q[3][0], (float)q[3][1]);
     r.z = make_float4((float)q[0][2], (float)q[1][2], (float)q[2][2], (float)q[3][2]);
-    r.fld = make_float4((float)p[0].w, (float)g[0], (float)g[1], (float)g[2]);
+    r.fld = make_float4((float)p[0].w, (float)p[1].w, (float)p[2].w, (float)p[3].w);
     r.nb = nb;
-    // condition gate: |grad|*diameter against the largest vertex value
-    double ext = 0, vmax = 0;
-#pragma unroll
-    for (int k = 1; k < 4; ++k)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) ext = fmax(ext, fabs(q[k][c] - q[0][c]));
-#pragma unroll
-    for (int k = 0; k < 4; ++k) vmax = fmax(vmax, fabs(p[k].w));
-    const double gn = fabs(g[0]) + fabs(g[1]) + fabs(g[2]);
-    const bool sliver = !(gn * ext <= 64.0 * vmax) || !isfinite(gn);
-    r.aux = make_int4(sliver ? kRec32Fp64Field : 0, 0, 0, 0);
+    r.aux = v;
     r32[t] = r;
   }
 }
@@ -362,16 +355,27 @@ dtfe_status_t mesh_upload(Mesh* m, const double* particle_data, int n, const int
   if (nt) SDTFE_CUDA(cudaMemcpyAsync(m->rows, tetra_data, sizeof(int4) * 2 * (size_t)nt, cudaMemcpyHostToDevice, s));
   SDTFE_CUDA(cudaMemsetAsync(m->stats, 0, sizeof(unsigned long long) * kStatCount, s));
   int* d_flags = nullptr;
-  SDTFE_CUDA(cudaMallocAsync(&d_flags, 2 * sizeof(int), s));
-  SDTFE_CUDA(cudaMemsetAsync(d_flags, 0, 2 * sizeof(int), s));
-  if (nt) k_validate<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, n, d_flags);
-  if (n) k_fp32_exact<<<grid_for(n), kBlock, 0, s>>>(m->pos, n, d_flags + 1);
-  int h_flags[2] = {0, 0};
+  SDTFE_CUDA(cudaMallocAsync(&d_flags, 3 * sizeof(int), s));
+  SDTFE_CUDA(cudaMemsetAsync(d_flags, 0, 3 * sizeof(int), s));
+  if (nt) {
+    k_validate<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, n, d_flags);
+    count_launch();
+  }
+  if (n) {
+    k_fp32_exact<<<grid_for(n), kBlock, 0, s>>>(m->pos, n, d_flags + 1, d_flags + 2);
+    count_launch();
+  }
+  int h_flags[3] = {0, 0, 0};
   SDTFE_CUDA(cudaMemcpyAsync(h_flags, d_flags, sizeof(h_flags), cudaMemcpyDeviceToHost, s));
   SDTFE_CUDA(cudaFreeAsync(d_flags, s));
   SDTFE_CUDA(cudaStreamSynchronize(s));
   SDTFE_CUDA(cudaGetLastError());
   m->fp32_exact = h_flags[1] == 0;
+  {
+    float mx;
+    memcpy(&mx, &h_flags[2], sizeof mx);
+    m->coord_max = (double)mx;
+  }
   if (h_flags[0])
     return set_error(DTFE_ERR_MESH, "tetra_data holds a vertex id outside [0, %d) or a neighbour id outside [-1, %d)", n, nt);
   m->has_density = (flags & DTFE_MESH_FIELD) != 0;
@@ -391,16 +395,23 @@ dtfe_status_t mesh_density(Mesh* m) {
   SDTFE_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (n + 1), s));
   if (nt) {
     k_volume<<<grid_for(nt), kBlock, 0, s>>>(m->pos, m->rows, nt, vol);
+    count_launch();
     k_count_tet_vertices<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, cnt);
+    count_launch();
   }
   SDTFE_TRY(exclusive_scan(cnt, off, n, s));
   SDTFE_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (n + 1), s));
-  if (nt) k_fill_tet_vertices<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, off, cnt, idx);
+  if (nt) {
+    k_fill_tet_vertices<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, off, cnt, idx);
+    count_launch();
+  }
   if (n) {
     k_sort_segments<<<grid_for(n), kBlock, 0, s>>>(off, n, idx);
+    count_launch();
     // p_mass*(1+DIM) is a float product in the reference (float * int)
     const double m4 = (double)(m->p_mass * 4);
     k_density<<<grid_for(n), kBlock, 0, s>>>(off, idx, vol, n, m4, m->pos, m->adj);
+    count_launch();
   }
   cudaFreeAsync(vol, s);
   cudaFreeAsync(cnt, s);
@@ -413,7 +424,10 @@ dtfe_status_t mesh_density(Mesh* m) {
 
 dtfe_status_t mesh_gradients(Mesh* m) {
   if (!m->grad) SDTFE_TRY(dmalloc(&m->grad, 3 * (size_t)m->nt, m));
-  if (m->nt) k_gradients<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->nt, m->grad);
+  if (m->nt) {
+    k_gradients<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->nt, m->grad);
+    count_launch();
+  }
   SDTFE_CUDA(cudaGetLastError());
   return DTFE_OK;
 }
@@ -425,9 +439,11 @@ dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32) {
   if (m->rec_axis == axis && (!want64 || have64) && (!want32 || have32)) return DTFE_OK;
   if (want64 && !m->rec64) SDTFE_TRY(dmalloc(&m->rec64, m->nt, m));
   if (want32 && !m->rec32) SDTFE_TRY(dmalloc(&m->rec32, m->nt, m));
-  if (m->nt)
+  if (m->nt) {
     k_records<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, axis,
                                                          m->rec64, m->rec32);
+    count_launch();
+  }
   SDTFE_CUDA(cudaGetLastError());
   m->rec_axis = axis;
   return DTFE_OK;
@@ -441,7 +457,10 @@ dtfe_status_t mesh_hull_mask(Mesh* m, int axis, uint32_t* host_mask_out, int* co
   SDTFE_CUDA(cudaMallocAsync(&mask, sizeof(uint32_t) * (nt ? nt : 1), s));
   SDTFE_CUDA(cudaMallocAsync(&cnt, sizeof(int) * (nt + 1), s));
   SDTFE_CUDA(cudaMallocAsync(&off, sizeof(int) * (nt + 1), s));
-  if (nt) k_hull_mask<<<grid_for(nt), kBlock, 0, s>>>(m->pos, m->rows, nt, axis, mask, cnt);
+  if (nt) {
+    k_hull_mask<<<grid_for(nt), kBlock, 0, s>>>(m->pos, m->rows, nt, axis, mask, cnt);
+    count_launch();
+  }
   SDTFE_TRY(exclusive_scan(cnt, off, nt, s));
   int total = 0;
   SDTFE_CUDA(cudaMemcpyAsync(&total, off + nt, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -478,6 +497,7 @@ dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count
     SDTFE_CUDA(cudaStreamSynchronize(s));
   } else if (nt) {
     k_hull_mask<<<grid_for(nt), kBlock, 0, s>>>(m->pos, m->rows, nt, axis, mask, cnt);
+    count_launch();
   }
   SDTFE_TRY(exclusive_scan(cnt, off, nt, s));
   int n_tri = 0;
@@ -497,19 +517,27 @@ dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count
   SDTFE_TRY(dmalloc(&A.tri, n_tri, m));
   SDTFE_TRY(dmalloc(&A.tri_rows, 8 * (size_t)n_tri, m));
   A.n_tri = n_tri;
-  if (nt) k_hull_emit<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, mask, off, A.tri_rows);
+  if (nt) {
+    k_hull_emit<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, mask, off, A.tri_rows);
+    count_launch();
+  }
   // vertex -> hull triangle lists for the edge matching
   int *vcnt = nullptr, *voff = nullptr, *vidx = nullptr;
   SDTFE_CUDA(cudaMallocAsync(&vcnt, sizeof(int) * (n + 1), s));
   SDTFE_CUDA(cudaMallocAsync(&voff, sizeof(int) * (n + 1), s));
   SDTFE_CUDA(cudaMallocAsync(&vidx, sizeof(int) * (3 * (size_t)n_tri + 1), s));
   SDTFE_CUDA(cudaMemsetAsync(vcnt, 0, sizeof(int) * (n + 1), s));
-  if (n_tri) k_count_tri_vertices<<<grid_for(n_tri), kBlock, 0, s>>>(A.tri_rows, n_tri, vcnt);
+  if (n_tri) {
+    k_count_tri_vertices<<<grid_for(n_tri), kBlock, 0, s>>>(A.tri_rows, n_tri, vcnt);
+    count_launch();
+  }
   SDTFE_TRY(exclusive_scan(vcnt, voff, n, s));
   SDTFE_CUDA(cudaMemsetAsync(vcnt, 0, sizeof(int) * (n + 1), s));
   if (n_tri) {
     k_fill_tri_vertices<<<grid_for(n_tri), kBlock, 0, s>>>(A.tri_rows, n_tri, voff, vcnt, vidx);
+    count_launch();
     k_hull_adjacency<<<grid_for(n_tri), kBlock, 0, s>>>(m->pos, axis, A.tri_rows, n_tri, voff, vidx, A.tri);
+    count_launch();
   }
   cudaFreeAsync(vcnt, s);
   cudaFreeAsync(voff, s);

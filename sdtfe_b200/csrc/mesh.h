@@ -16,6 +16,9 @@ namespace sdtfe {
 // thread-local last error (capi.cu)
 dtfe_status_t set_error(dtfe_status_t s, const char* fmt, ...);
 
+// process-wide count of kernels this library has launched (capi.cu)
+void count_launch(unsigned n = 1);
+
 #define SDTFE_CUDA(expr)                                                                  \
   do {                                                                                    \
     cudaError_t e_ = (expr);                                                              \
@@ -54,6 +57,7 @@ struct Mesh {
   unsigned flags = 0;
   bool fp32_exact = false;
   bool has_density = false;
+  double coord_max = 0;     // largest |x|, |y|, |z| of any vertex (rounded up)
   cudaStream_t stream = nullptr;
   double4* pos = nullptr;   // (x, y, z, rho) in the original frame
   int4* rows = nullptr;     // 2 per tet: vertex ids, neighbour ids
@@ -66,6 +70,7 @@ struct Mesh {
   unsigned long long* stats = nullptr;  // kStatCount counters of the last map
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool timed = false;       // ev0/ev1 bracket the last walk launch
+  int tune32 = -1;          // mixed-map kernel variant chosen by the autotuner (-1: default)
   size_t bytes = 0;
 };
 
@@ -113,6 +118,8 @@ dtfe_status_t launch_trace32(Mesh& m, int n_rays, const double* d_x, const doubl
                              double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
                              int* d_crossed, int* d_status, int* d_visits, int max_record,
                              cudaStream_t s);
+int num_map32_variants();
+void map32_variant_info(int i, int* block, int* minb, int* wide);
 dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
                             uint64_t seed, int max_visits, double* d_grid, cudaStream_t s);
 

@@ -241,6 +241,7 @@ dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
   SDTFE_CUDA(cudaEventRecord(m.ev0, s));
   k_map64<<<(unsigned)blocks, threads, smem, s>>>(a);
+  count_launch();
   SDTFE_CUDA(cudaGetLastError());
   SDTFE_CUDA(cudaEventRecord(m.ev1, s));
   m.timed = true;
@@ -253,10 +254,12 @@ dtfe_status_t launch_trace64(Mesh& m, int n_rays, const double* d_x, const doubl
                              cudaStream_t s) {
   const AxisData& A = m.ax[m.rec_axis];
   WalkConf64 w{lz, (dxy / 2.0) / kPerturbMax, seed, max_visits};
-  if (n_rays > 0)
+  if (n_rays > 0) {
     k_trace64<<<(n_rays + 127) / 128, 128, 0, s>>>(m.rec64, A.tri, A.n_tri, n_rays, d_x, d_y, z0, w,
                                                    4 * A.n_tri + 64, d_rho, d_crossed, d_status,
                                                    d_visits, max_record);
+    count_launch();
+  }
   SDTFE_CUDA(cudaGetLastError());
   return DTFE_OK;
 }
@@ -275,6 +278,7 @@ dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[
   k_grid64<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(m.rec64, A.tri, A.n_tri, G, dxy, offx,
                                                           offy, offz, box_len, (int)ss, w,
                                                           4 * A.n_tri + 64, d_grid, m.stats);
+  count_launch();
   SDTFE_CUDA(cudaGetLastError());
   SDTFE_CUDA(cudaEventRecord(m.ev1, s));
   m.timed = true;

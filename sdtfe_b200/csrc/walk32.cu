@@ -1,22 +1,688 @@
-// walk32.cu - mixed-precision surface-density map (FP32 walk, guarded FP64).
+// walk32.cu - mixed-precision surface-density map: FP32 walk, guarded FP64.
+//
+// What stays exact.  The walk's topology (which faces the ray enters and
+// leaves, when it perturbs, which tet comes next) depends only on the signs
+// of six Plücker products per tet, thresholded at ZERO as the reference does
+// (src/dtfe.c:19-21).  Each product is evaluated in FP32 from coordinates
+// taken relative to the ray origin (the origin split into a float hi/lo
+// pair) together with a bound on its FP32 error.  When every product clears
+// the reference's threshold by more than that bound plus the reference's own
+// FP64 rounding, all six reference signs are known and nonzero, and a 64-entry
+// table maps them to the reference's enter/leave choice.  Otherwise the tet
+// is re-tested with the reference's FP64 products and operands and the
+// general face rule (zero signs, perturbation) applies, exactly as in the FP64
+// walk.  Every ray therefore visits the FP64 path's tets in the FP64 path's
+// order.
+//
+// What is FP32.  The integral.  Only the exit crossing of each tet is
+// computed: its position is vertex A's z plus a barycentric offset (weights =
+// the exit face's signed edge terms over their sum; the terms share one sign,
+// so there is no cancellation) and its field value is the same barycentric
+// mix of the face's vertex densities.  Both are carried into the next tet as
+// its entry crossing, so consecutive chords share their interface exactly and
+// the chord lengths telescope: an ill-conditioned face (nearly parallel to
+// the ray) only moves an interface, which the continuity of the linear field
+// makes a second-order effect.  The chord contributes (f_in + f_out)/2 times
+// its length - exact for the linear field, and the reference's value
+// (rho_A + grad.(p_mid - v_A)) * dz (src/dtfe.c:356-369) in exact arithmetic.
+// Crossing positions and the ray's sum are FP64 (a float vertex z plus a float
+// offset, added exactly; one multiply-add per chord).  The midpoint-in-slab
+// test uses a guard band; inside it the reference's FP64 midpoint decides.  A tet whose entry face is not the face it was reached
+// through (turn-arounds, perturbations) computes its own entry crossing, as
+// the reference does.
+//
+// Compiled with -fmad=false like walk.cu: the sample positions and the point
+// location it shares with the FP64 walk must round as the reference does;
+// the FP32 arithmetic asks for fused multiply-adds explicitly.
+#include <cfloat>
+
 #include "mesh.h"
 
 namespace sdtfe {
 
+namespace {
+
+constexpr float kEps = 5.9604645e-08f;  // 2^-24, FP32 unit roundoff
+
+struct MixConf {
+  double lz;          // slab depth (the reference's ray length)
+  double z0d, z1d;    // slab bounds
+  float z0, z1;       // slab bounds rounded to float (compared with a guard band)
+  double thr;         // the reference's ZERO in units of lz
+  double coord_max;   // largest vertex coordinate magnitude
+  double coord_err;   // rounding of the float records (0 when they are exact)
+  double dist;        // perturbation step
+  uint64_t seed;
+  int max_visits;
+  const TetRec64* __restrict__ rec64;  // exact coordinates when the floats are not
+  int exact32;                         // the float coordinates are the doubles
+};
+
+struct RayState {
+  double ox, oy;     // ray origin (perturbed in place)
+  float oxh, oxl, oyh, oyl;
+  float thr_hi;      // the reference's threshold plus its own error, in units of lz
+  float e_coef;      // error of the products per unit of the tet's largest |relative coordinate|
+};
+
+// Float hi/lo split of the origin and this ray's filter constants.  The
+// reference's own FP64 error on a product is at most 8 roundings of
+// magnitude <= 6*M^2*lz (M: largest coordinate or origin magnitude), i.e.
+// 48*2^-53*M^2 in units of lz.  A relative coordinate carries at most
+// 3*eps^2*|o| from the split plus the records' rounding (e_abs); on a product
+// that is at most 2*e_abs*(|px|+|py|+|qx|+|qy|) <= 8*e_abs*Dmax.
+__device__ __forceinline__ void ray_setup(RayState& r, const MixConf& C) {
+  r.oxh = (float)r.ox;
+  r.oxl = (float)(r.ox - (double)r.oxh);
+  r.oyh = (float)r.oy;
+  r.oyl = (float)(r.oy - (double)r.oyh);
+  const double M = fmax(C.coord_max, fmax(fabs(r.ox), fabs(r.oy)));
+  const double ref_err = 32.0 * DBL_EPSILON * M * M + 1e-300;
+  r.thr_hi = __double2float_ru((C.thr + ref_err) * (1.0 + 1e-5));
+  const double eps = 5.9604644775390625e-08;
+  const double e_abs = 4.0 * eps * eps * (fabs(r.ox) + fabs(r.oy)) + C.coord_err;
+  r.e_coef = __double2float_ru(8.0 * 1.01 * e_abs) + FLT_MIN;
+}
+
+struct Verts32 {
+  float x[4], y[4];  // absolute (projected frame)
+  float z[4];
+  float rho[4];
+};
+
+__device__ __forceinline__ void load32(const TetRec32* __restrict__ R, int t, Verts32& v,
+                                       int4& nb) {
+  const TetRec32* p = R + t;
+  const float4 a = __ldg(&p->xyab), b = __ldg(&p->xycd), z = __ldg(&p->z), f = __ldg(&p->fld);
+  nb = __ldg(&p->nb);
+  v.x[0] = a.x; v.y[0] = a.y; v.x[1] = a.z; v.y[1] = a.w;
+  v.x[2] = b.x; v.y[2] = b.y; v.x[3] = b.z; v.y[3] = b.w;
+  v.z[0] = z.x; v.z[1] = z.y; v.z[2] = z.z; v.z[3] = z.w;
+  v.rho[0] = f.x; v.rho[1] = f.y; v.rho[2] = f.z; v.rho[3] = f.w;
+}
+
+// Exact double coordinates of vertex k of tet t, fetched from memory (the
+// float record when its floats are the doubles, else the FP64 record).
+__device__ __forceinline__ double2 xy64_at(const TetRec32* __restrict__ R32,
+                                           const TetRec64* __restrict__ R64, int exact32, int t,
+                                           int k) {
+  if (exact32) {
+    const float4 q = __ldg(k < 2 ? &R32[t].xyab : &R32[t].xycd);
+    return (k & 1) ? make_double2(q.z, q.w) : make_double2(q.x, q.y);
+  }
+  return __ldg(&R64[t].xy[k]);
+}
+
+__device__ __forceinline__ double z64_at(const TetRec32* __restrict__ R32,
+                                         const TetRec64* __restrict__ R64, int exact32, int t,
+                                         int k) {
+  if (exact32) {
+    const float4 z = __ldg(&R32[t].z);
+    return (double)sel4(k, z.x, z.y, z.z, z.w);
+  }
+  const double2 zz = __ldg(k < 2 ? &R64[t].zab : &R64[t].zcd);
+  return (k & 1) ? zz.y : zz.x;
+}
+
+// The reference's FP64 product for edge P->Q, operands and order as in
+// src/dtfe.c:24-26.
+__device__ __forceinline__ double edge_u64_exact(double lz, double ox, double oy, double2 p,
+                                                 double2 q) {
+  const double v0 = __dsub_rn(p.x, q.x);
+  const double v1 = __dsub_rn(p.y, q.y);
+  const double v5 = __dsub_rn(__dmul_rn(p.x, q.y), __dmul_rn(p.y, q.x));
+  const double m_oy = __dmul_rn(-lz, oy);
+  const double ox_l = __dmul_rn(lz, ox);
+  return __dadd_rn(__dadd_rn(__dmul_rn(lz, v5), __dmul_rn(v0, m_oy)), __dmul_rn(v1, ox_l));
+}
+
+// edges CB, AC, BA, DC, BD, DA as P -> Q vertex slots (inside unrolled loops)
+#define SDTFE_EDGE_TABLES                       \
+  constexpr int kEdgeP[6] = {2, 2, 1, 2, 1, 3}; \
+  constexpr int kEdgeQ[6] = {1, 0, 0, 3, 3, 0};
+
+// Slow path: the reference's six signs for tet t, packed 2 bits per edge
+// (0: zero, 1: positive, 2: negative).
+__device__ __noinline__ unsigned exact_signs(const TetRec32* __restrict__ R32,
+                                             const TetRec64* __restrict__ R64, int exact32,
+                                             double lz, int t, double ox, double oy) {
+  SDTFE_EDGE_TABLES
+  double2 xy[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) xy[k] = xy64_at(R32, R64, exact32, t, k);
+  unsigned packed = 0;
+#pragma unroll
+  for (int e = 0; e < 6; ++e) {
+    const int s = sign_eps(edge_u64_exact(lz, ox, oy, xy[kEdgeP[e]], xy[kEdgeQ[e]]));
+    packed |= (unsigned)(s > 0 ? 1 : (s < 0 ? 2 : 0)) << (2 * e);
+  }
+  return packed;
+}
+
+// Face choice from six certain (nonzero) signs.  neg has bit e set when edge e
+// (CB, AC, BA, DC, BD, DA) is negative; entry = enter | leave << 2 | ok << 4,
+// the reference's first-entered / first-left rule (src/dtfe.c:66-213) with
+// faces in the order BDC, ACD, ADB, ABC.
+__host__ __device__ constexpr unsigned face_lut_entry(unsigned neg) {
+  const bool e0 = (neg & 25u) == 17u, e1 = (neg & 42u) == 40u, e2 = (neg & 52u) == 4u,
+             e3 = (neg & 7u) == 2u;
+  const bool l0 = (neg & 25u) == 8u, l1 = (neg & 42u) == 2u, l2 = (neg & 52u) == 48u,
+             l3 = (neg & 7u) == 5u;
+  const int en = e0 ? 0 : (e1 ? 1 : (e2 ? 2 : (e3 ? 3 : -1)));
+  const int le = l0 ? 0 : (l1 ? 1 : (l2 ? 2 : (l3 ? 3 : -1)));
+  return (en >= 0 && le >= 0) ? ((unsigned)en | (unsigned)le << 2 | 16u) : 0u;
+}
+
+struct Hit32 {
+  int enter, leave;
+  bool ok, special;
+};
+
+// The filtered test of one tet.  u[] receives the FP32 products (units of lz).
+__device__ __forceinline__ Hit32 tet_test(const TetRec32* __restrict__ R32, const MixConf& C,
+                                          const RayState& r, int t, const Verts32& v, float u[6],
+                                          float* bmax, const unsigned char* __restrict__ lut,
+                                          int* fallbacks) {
+  SDTFE_EDGE_TABLES
+  float dx[4], dy[4];
+  float dmax = 0.f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    dx[k] = __fsub_rn(__fsub_rn(v.x[k], r.oxh), r.oxl);
+    dy[k] = __fsub_rn(__fsub_rn(v.y[k], r.oyh), r.oyl);
+    dmax = fmaxf(dmax, fmaxf(fabsf(dx[k]), fabsf(dy[k])));
+  }
+  // one bound for the tet's six products: |ue - u'| <= 6 eps (|a| + |b|)
+  // + 2 e_abs sum|d| with |a|, |b| <= dmax^2; 48 eps dmax^2 is 4x the first
+  // term, e_coef dmax covers the second, thr_hi is the reference's threshold
+  const float bound = __fmaf_ru(48.f * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
+  unsigned neg = 0, unc = 0;
+#pragma unroll
+  for (int e = 0; e < 6; ++e) {
+    const float px = dx[kEdgeP[e]], py = dy[kEdgeP[e]], qx = dx[kEdgeQ[e]], qy = dy[kEdgeQ[e]];
+    const float ue = __fsub_rn(__fmul_rn(px, qy), __fmul_rn(py, qx));
+    unc |= (fabsf(ue) <= bound ? 1u : 0u) << e;
+    neg |= (__float_as_uint(ue) >> 31) << e;
+    u[e] = ue;
+  }
+  *bmax = bound;
+  Hit32 h;
+  if (unc == 0) {
+    const unsigned ent = lut[neg];
+    h.enter = (int)(ent & 3u);
+    h.leave = (int)((ent >> 2) & 3u);
+    h.ok = (ent & 16u) != 0;
+    h.special = false;
+    return h;
+  }
+  // some product is too close to the reference's threshold: the reference decides
+  *fallbacks += __popc(unc);
+  const unsigned pk = exact_signs(R32, C.rec64, C.exact32, C.lz, t, r.ox, r.oy);
+  int s[6];
+#pragma unroll
+  for (int e = 0; e < 6; ++e) {
+    const unsigned c = (pk >> (2 * e)) & 3u;
+    s[e] = c == 1u ? 1 : (c == 2u ? -1 : 0);
+  }
+  const Hit64 g = plucker_faces(s);
+  h.enter = g.enter;
+  h.leave = g.leave;
+  h.ok = g.ok;
+  h.special = g.special;
+  return h;
+}
+
+// Where the ray crosses face f (face f lies opposite vertex f): offset of the
+// crossing's z from vertex A's z, and the field value there.  Each corner's
+// weight is the signed term of the face edge opposite it over their sum.
+// Returns a bound on the weights' error (three times the tet's product bound
+// over |sum|): large for a face nearly parallel to the ray.
+__device__ __forceinline__ float crossing(int f, const float u[6], float bmax, const Verts32& v,
+                                          float* dz, float* fv) {
+  // u: CB=0, AC=1, BA=2, DC=3, BD=4, DA=5
+  const float wa = sel4(f, 0.f, -u[3], u[4], u[0]);
+  const float wb = sel4(f, u[3], 0.f, u[5], -u[1]);
+  const float wc = sel4(f, -u[4], -u[5], 0.f, u[2]);
+  const float wd = sel4(f, -u[0], u[1], -u[2], 0.f);
+  const float den = wa + wb + wc + wd;
+  const float r = __fdividef(1.f, den);
+  const float zb = v.z[1] - v.z[0], zc = v.z[2] - v.z[0], zd = v.z[3] - v.z[0];
+  *dz = r * __fmaf_rn(wd, zd, __fmaf_rn(wc, zc, wb * zb));
+  *fv = r * __fmaf_rn(wd, v.rho[3], __fmaf_rn(wc, v.rho[2], __fmaf_rn(wb, v.rho[1], wa * v.rho[0])));
+  return 3.f * bmax * fabsf(r);
+}
+
+// Crossing of face f of tet t computed from the exact operands: the
+// reference's FP64 point (face_z64) and the FP64 barycentric field value.
+// Used where a crossing is not shared with a neighbouring chord (the ray's
+// entry into and exit from the mesh, a re-entry after a perturbation or a
+// turn-around) and where the FP32 weights are ill-conditioned.
+__device__ __noinline__ double2 exact_crossing(const TetRec32* __restrict__ R32,
+                                               const TetRec64* __restrict__ R64, int exact32,
+                                               double lz, int t, int f, double ox, double oy) {
+  SDTFE_EDGE_TABLES
+  double2 xy[4];
+  double z[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    xy[k] = xy64_at(R32, R64, exact32, t, k);
+    z[k] = z64_at(R32, R64, exact32, t, k);
+  }
+  double u[6];
+#pragma unroll
+  for (int e = 0; e < 6; ++e) u[e] = edge_u64_exact(lz, ox, oy, xy[kEdgeP[e]], xy[kEdgeQ[e]]);
+  const double zc = face_z64(f, u, z);
+  const float4 rho = __ldg(&R32[t].fld);
+  const double wa = sel4(f, 0.0, -u[3], u[4], u[0]);
+  const double wb = sel4(f, u[3], 0.0, u[5], -u[1]);
+  const double wc = sel4(f, -u[4], -u[5], 0.0, u[2]);
+  const double wd = sel4(f, -u[0], u[1], -u[2], 0.0);
+  const double fv = (wa * rho.x + wb * rho.y + wc * rho.z + wd * rho.w) / (wa + wb + wc + wd);
+  return make_double2(zc, fv);
+}
+
+// weights error above which a crossing is recomputed in FP64 (2^-12)
+constexpr float kCrossingTol = 2.44140625e-4f;
+
+// The reference's FP64 chord midpoint for the chosen faces (slab-test guard).
+__device__ __noinline__ double midpoint64(const TetRec32* __restrict__ R32,
+                                          const TetRec64* __restrict__ R64, int exact32, double lz,
+                                          int t, int enter, int leave, double ox, double oy) {
+  SDTFE_EDGE_TABLES
+  double2 xy[4];
+  double z[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    xy[k] = xy64_at(R32, R64, exact32, t, k);
+    z[k] = z64_at(R32, R64, exact32, t, k);
+  }
+  double u[6];
+#pragma unroll
+  for (int e = 0; e < 6; ++e) u[e] = edge_u64_exact(lz, ox, oy, xy[kEdgeP[e]], xy[kEdgeQ[e]]);
+  const double zi = face_z64(enter, u, z), zo = face_z64(leave, u, z);
+  const double d = zo - zi;
+  return d / 2 + zi;
+}
+
+// One chord's contribution: (f_in + f_out)/2 times its length when its
+// midpoint lies in the slab (src/dtfe.c:356-369).  Crossing positions are
+// doubles (a float vertex z plus a float offset, summed exactly), so the exit
+// of one chord is bit-for-bit the entry of the next and the chord lengths
+// telescope.  The slab test compares the float midpoint with a guard band;
+// inside the band the reference's FP64 midpoint decides.
+__device__ __forceinline__ double chord32(const TetRec32* __restrict__ R, const MixConf& C,
+                                          const RayState& r, int t, int enter, int leave,
+                                          double z_in, float f_in, double z_out, float f_out,
+                                          float hz, int* fallbacks) {
+  const double d = z_out - z_in;
+  const float zm = (float)(z_in + 0.5 * d);
+  const float guard = 64.f * kEps * (fabsf(zm) + hz);
+  bool inside;
+  if (fabsf(zm - C.z0) > guard && fabsf(zm - C.z1) > guard) {
+    inside = zm > C.z0 && zm < C.z1;
+  } else {
+    const double zmd = midpoint64(R, C.rec64, C.exact32, C.lz, t, enter, leave, r.ox, r.oy);
+    inside = zmd > C.z0d && zmd < C.z1d;
+    ++*fallbacks;
+  }
+  return inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
+}
+
+// The mixed walk.  Same control flow as walk64 (src/dtfe.c:247-374); returns
+// the status, the integral in *rho and the crossing count.
+__device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixConf& C, int ft,
+                                      double x, double y, uint64_t ray,
+                                      const unsigned char* __restrict__ lut, double* rho_out,
+                                      int* crossed_out, int* fallbacks_out, int* visits,
+                                      int max_record) {
+  *crossed_out = 0;
+  *rho_out = 0.0;
+  *fallbacks_out = 0;
+  if (ft < 0) return kRayMiss;
+  RayState r;
+  r.ox = x;
+  r.oy = y;
+  ray_setup(r, C);
+  uint64_t ctr = 0;
+  double sum = 0.0, z_in = 0.0;
+  float f_in = 0.f;
+  bool carried = false;  // z_in / f_in hold the previous tet's exit crossing
+  int crossed = 0, fallbacks = 0;
+  int4 nb = make_int4(ft, -1, -1, -1);
+  int leave = 0, enter = -1;
+  int cur = ft, prev = -1;
+  for (;;) {
+    int nx = nb_at(nb, leave);
+    if (nx == -1) break;
+    if (nx == prev) {
+      const int t = enter;
+      enter = leave;
+      leave = t;
+      nx = nb_at(nb, leave);
+      if (nx == -1) break;
+    }
+    prev = cur;
+    cur = nx;
+    if (crossed >= C.max_visits) {
+      *fallbacks_out = fallbacks;
+      return kRayBudget;
+    }
+    Verts32 v;
+    load32(R, cur, v, nb);
+    float u[6], bmax;
+    Hit32 h = tet_test(R, C, r, cur, v, u, &bmax, lut, &fallbacks);
+    if (!h.ok) {
+      *fallbacks_out = fallbacks;
+      return kRayNoExit;
+    }
+    int np = 0;
+    while (h.special) {  // FP64 perturbation, exactly as the reference (src/dtfe.c:219-245)
+      const int k = sdtfe_rand31(C.seed, ray, ctr++) % 4;
+      const double2 vk = xy64_at(R, C.rec64, C.exact32, cur, k);
+      double dx = __dsub_rn(vk.x, r.ox);
+      double dy = __dsub_rn(vk.y, r.oy);
+      const double mag = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+      if (mag > C.dist) {
+        dx = __ddiv_rn(dx, mag);
+        dy = __ddiv_rn(dy, mag);
+        dx = __dmul_rn(dx, C.dist);
+        dy = __dmul_rn(dy, C.dist);
+      }
+      r.ox = __dadd_rn(r.ox, dx);
+      r.oy = __dadd_rn(r.oy, dy);
+      ray_setup(r, C);
+      carried = false;  // the ray moved: this tet computes its own entry
+      if (++np > kPerturbMax) {
+        *fallbacks_out = fallbacks;
+        return kRayPerturbMax;
+      }
+      h = tet_test(R, C, r, cur, v, u, &bmax, lut, &fallbacks);
+      if (!h.ok) {
+        *fallbacks_out = fallbacks;
+        return kRayNoExit;
+      }
+    }
+    enter = h.enter;
+    leave = h.leave;
+    if (visits != nullptr && crossed < max_record) visits[crossed] = cur;
+    ++crossed;
+
+    // entry crossing: carried over from the previous chord, or computed from
+    // the exact operands where it is not shared (first tet, perturbation,
+    // turn-around)
+    if (!carried || nb_at(nb, enter) != prev) {
+      const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, enter, r.ox, r.oy);
+      z_in = c.x;
+      f_in = (float)c.y;
+      ++fallbacks;
+    }
+    // exit crossing: FP32 unless it leaves the mesh (not shared with a
+    // neighbouring chord) or is ill-conditioned
+    float dzo, f_out;
+    double z_out;
+    const float cond = crossing(leave, u, bmax, v, &dzo, &f_out);
+    if (nb_at(nb, leave) == -1 || !(cond <= kCrossingTol)) {
+      const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
+      z_out = c.x;
+      f_out = (float)c.y;
+      ++fallbacks;
+    } else {
+      z_out = (double)v.z[0] + (double)dzo;
+    }
+    const float hz = fmaxf(fmaxf(fabsf(v.z[1] - v.z[0]), fabsf(v.z[2] - v.z[0])),
+                           fabsf(v.z[3] - v.z[0]));
+    sum += chord32(R, C, r, cur, enter, leave, z_in, f_in, z_out, f_out, hz, &fallbacks);
+    z_in = z_out;
+    f_in = f_out;
+    carried = true;
+  }
+  *crossed_out = crossed;
+  *rho_out = sum;
+  *fallbacks_out = fallbacks;
+  return kRayOk;
+}
+
+__device__ __forceinline__ void fill_lut(unsigned char* lut) {
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) lut[i] = (unsigned char)face_lut_entry(i);
+}
+
+struct MapArgs32 {
+  const TetRec32* __restrict__ rec;
+  const TriRec64* __restrict__ tri;
+  int n_tri;
+  double* __restrict__ map;
+  int G, S, TW, TH, tiles_x;
+  double dxy, offx, offy, scale, soff;
+  MixConf C;
+  int loc_budget;
+  unsigned long long* __restrict__ stats;
+  double* __restrict__ ray_rho;
+  int* __restrict__ ray_crossed;
+  int* __restrict__ ray_status;
+};
+
+__device__ __forceinline__ void add_stats32(unsigned long long* stats, bool active, int crossed,
+                                            int status, int fallbacks) {
+  const unsigned mask = __activemask();
+  const unsigned rr = __reduce_add_sync(mask, active ? 1u : 0u);
+  const unsigned vv = __reduce_add_sync(mask, active ? (unsigned)crossed : 0u);
+  const unsigned fb = __reduce_add_sync(mask, active ? (unsigned)fallbacks : 0u);
+  unsigned st[DTFE_N_RAY_STATUS];
+#pragma unroll
+  for (int k = 0; k < DTFE_N_RAY_STATUS; ++k)
+    st[k] = __reduce_add_sync(mask, (active && status == k) ? 1u : 0u);
+  if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) {
+    if (rr) atomicAdd(stats + kStatRays, (unsigned long long)rr);
+    if (vv) atomicAdd(stats + kStatVisits, (unsigned long long)vv);
+    if (fb) atomicAdd(stats + kStatFallback, (unsigned long long)fb);
+#pragma unroll
+    for (int k = 0; k < DTFE_N_RAY_STATUS; ++k)
+      if (st[k]) atomicAdd(stats + kStatStatus0 + k, (unsigned long long)st[k]);
+  }
+}
+
+// Same tiling as k_map64: block = tile of pixels x samples, pixel means in
+// sample order from shared memory.  BLOCK threads per block and MINB blocks
+// per SM (the register budget) are compile-time; the autotuner picks among
+// the instantiations.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_map32(const MapArgs32 a) {
+  extern __shared__ double s_val32[];  // P*S doubles, then P*S success bytes
+  __shared__ unsigned char s_lut[64];
+  fill_lut(s_lut);
+  __syncthreads();
+  const int P = a.TW * a.TH;
+  unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + P * a.S);
+  const int tile = blockIdx.x;
+  const int tx0 = (tile % a.tiles_x) * a.TW, ty0 = (tile / a.tiles_x) * a.TH;
+  for (int t = threadIdx.x; t < P * a.S; t += BLOCK) {
+    const int lp = t / a.S, s = t % a.S;
+    const int col = tx0 + lp % a.TW, row = ty0 + lp / a.TW;
+    const bool active = col < a.G && row < a.G;
+    double v = 0.0;
+    int crossed = 0, status = kRayMiss, fb = 0;
+    if (active) {
+      const long long p = (long long)row * a.G + col;
+      const double x = col * a.dxy + a.offx - a.soff;
+      const double y = row * a.dxy + a.offy - a.soff;
+      const double xt = x + sdtfe_sample_u01(a.C.seed, (uint64_t)p, (uint32_t)s, 0) * a.scale;
+      const double yt = y + sdtfe_sample_u01(a.C.seed, (uint64_t)p, (uint32_t)s, 1) * a.scale;
+      const uint64_t rid = (uint64_t)p * (uint64_t)a.S + (uint64_t)s;
+      int ft = -1;
+      if (a.n_tri > 0) ft = locate64(a.tri, 0, xt, yt, a.loc_budget, &status);
+      if (ft >= 0)
+        status = walk32(a.rec, a.C, ft, xt, yt, rid, s_lut, &v, &crossed, &fb, nullptr, 0);
+      if (status != kRayOk) v = 0.0;
+      if (a.ray_rho) {
+        a.ray_rho[rid] = v;
+        a.ray_crossed[rid] = crossed;
+        a.ray_status[rid] = status;
+      }
+    }
+    s_val32[t] = v;
+    s_ok[t] = crossed > 0;
+    add_stats32(a.stats, active, crossed, status, fb);
+  }
+  __syncthreads();
+  for (int lp = threadIdx.x; lp < P; lp += BLOCK) {
+    const int col = tx0 + lp % a.TW, row = ty0 + lp / a.TW;
+    if (col >= a.G || row >= a.G) continue;
+    double total = 0.0;
+    int n_avg = 0;
+    for (int s = 0; s < a.S; ++s) {
+      total += s_val32[lp * a.S + s];
+      n_avg += s_ok[lp * a.S + s];
+    }
+    a.map[(size_t)row * a.G + col] += n_avg > 0 ? total / n_avg : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_trace32(const TetRec32* __restrict__ rec,
+                                                 const TriRec64* __restrict__ tri, int n_tri,
+                                                 int n_rays, const double* __restrict__ xs,
+                                                 const double* __restrict__ ys, MixConf C,
+                                                 int loc_budget, double* __restrict__ rho,
+                                                 int* __restrict__ crossed,
+                                                 int* __restrict__ status,
+                                                 int* __restrict__ visits, int max_record) {
+  __shared__ unsigned char s_lut[64];
+  fill_lut(s_lut);
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_rays) return;
+  int st = kRayMiss, c = 0, fb = 0;
+  double v = 0.0;
+  const int ft = n_tri > 0 ? locate64(tri, 0, xs[i], ys[i], loc_budget, &st) : -1;
+  if (ft >= 0)
+    st = walk32(rec, C, ft, xs[i], ys[i], (uint64_t)i, s_lut, &v, &c, &fb,
+                visits ? visits + (size_t)i * max_record : nullptr, max_record);
+  rho[i] = st == kRayOk ? v : 0.0;
+  crossed[i] = c;
+  status[i] = st;
+}
+
+MixConf mix_conf(const Mesh& m, double z0, double lz, double dist, uint64_t seed,
+                 int max_visits) {
+  MixConf C;
+  C.lz = lz;
+  C.z0d = z0;
+  C.z1d = z0 + lz;
+  C.z0 = (float)C.z0d;
+  C.z1 = (float)C.z1d;
+  C.thr = kZero / lz;
+  C.coord_max = m.coord_max;
+  C.coord_err = m.fp32_exact ? 0.0 : 5.9604644775390625e-08 * m.coord_max;
+  C.dist = dist;
+  C.seed = seed;
+  C.max_visits = max_visits;
+  C.rec64 = m.rec64;
+  C.exact32 = m.fp32_exact ? 1 : 0;
+  return C;
+}
+
+// Pixels per block = threads / samples, laid out square-ish (wide = 0) or as
+// a row strip (wide = 1).
+void tile_shape32(int threads, int S, int wide, int* TW, int* TH) {
+  int P = threads / S;
+  if (P < 1) P = 1;
+  if (wide) {
+    *TW = P;
+    *TH = 1;
+    return;
+  }
+  const int lg = 31 - __builtin_clz((unsigned)P);
+  const int tw = 1 << ((lg + 1) / 2);
+  const int th = P / tw;
+  *TW = tw;
+  *TH = th < 1 ? 1 : th;
+}
+
+typedef void (*MapKernel32)(const MapArgs32);
+
+struct Variant32 {
+  MapKernel32 kernel;
+  int block, minb, wide;
+};
+
+const Variant32 kVariants32[] = {
+    {k_map32<256, 2>, 256, 2, 0}, {k_map32<256, 3>, 256, 3, 0}, {k_map32<256, 4>, 256, 4, 0},
+    {k_map32<128, 4>, 128, 4, 0}, {k_map32<128, 6>, 128, 6, 0}, {k_map32<256, 2>, 256, 2, 1},
+    {k_map32<256, 3>, 256, 3, 1},
+};
+constexpr int kNumVariants32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
+constexpr int kDefaultVariant32 = 1;  // (256, 3): the usual winner on B200
+
+}  // namespace
+
 dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
                            double* ray_rho, int* ray_crossed, int* ray_status) {
-  (void)m; (void)g; (void)d_map; (void)s; (void)ray_rho; (void)ray_crossed; (void)ray_status;
-  return set_error(DTFE_ERR_UNSUPPORTED, "mixed-precision map not built yet");
+  if (!m.rec32) return set_error(DTFE_ERR_INVALID, "mixed map without FP32 records");
+  if (!m.fp32_exact && !m.rec64)
+    return set_error(DTFE_ERR_INVALID, "coordinates are not floats and no FP64 records are kept");
+  const AxisData& A = m.ax[m.rec_axis];
+  const int vi = (m.tune32 >= 0 && m.tune32 < kNumVariants32) ? m.tune32 : kDefaultVariant32;
+  const Variant32& V = kVariants32[vi];
+  MapArgs32 a;
+  a.rec = m.rec32;
+  a.tri = A.tri;
+  a.n_tri = A.n_tri;
+  a.map = d_map;
+  a.G = g.G;
+  a.S = g.S;
+  tile_shape32(V.block, g.S, V.wide, &a.TW, &a.TH);
+  a.tiles_x = (g.G + a.TW - 1) / a.TW;
+  const int tiles_y = (g.G + a.TH - 1) / a.TH;
+  a.dxy = g.dxy;
+  a.offx = g.offx;
+  a.offy = g.offy;
+  a.scale = g.scale;
+  a.soff = g.soff;
+  a.C = mix_conf(m, g.offz, g.lz, g.dist, g.seed, g.max_visits);
+  a.loc_budget = 4 * A.n_tri + 64;
+  a.stats = m.stats;
+  a.ray_rho = ray_rho;
+  a.ray_crossed = ray_crossed;
+  a.ray_status = ray_status;
+  const size_t smem = (size_t)a.TW * a.TH * g.S * (sizeof(double) + 1);
+  if (smem > 40 * 1024)
+    SDTFE_CUDA(cudaFuncSetAttribute(V.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long blocks = (long long)a.tiles_x * tiles_y;
+  SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
+  SDTFE_CUDA(cudaEventRecord(m.ev0, s));
+  V.kernel<<<(unsigned)blocks, V.block, smem, s>>>(a);
+  count_launch();
+  SDTFE_CUDA(cudaGetLastError());
+  SDTFE_CUDA(cudaEventRecord(m.ev1, s));
+  m.timed = true;
+  return DTFE_OK;
 }
 
 dtfe_status_t launch_trace32(Mesh& m, int n_rays, const double* d_x, const double* d_y, double z0,
                              double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
                              int* d_crossed, int* d_status, int* d_visits, int max_record,
                              cudaStream_t s) {
-  (void)m; (void)n_rays; (void)d_x; (void)d_y; (void)z0; (void)lz; (void)dxy; (void)seed;
-  (void)max_visits; (void)d_rho; (void)d_crossed; (void)d_status; (void)d_visits; (void)max_record;
-  (void)s;
-  return set_error(DTFE_ERR_UNSUPPORTED, "mixed-precision trace not built yet");
+  if (!m.rec32) return set_error(DTFE_ERR_INVALID, "mixed trace without FP32 records");
+  if (!m.fp32_exact && !m.rec64)
+    return set_error(DTFE_ERR_INVALID, "coordinates are not floats and no FP64 records are kept");
+  const AxisData& A = m.ax[m.rec_axis];
+  MixConf C = mix_conf(m, z0, lz, (dxy / 2.0) / kPerturbMax, seed, max_visits);
+  if (n_rays > 0) {
+    k_trace32<<<(n_rays + 127) / 128, 128, 0, s>>>(m.rec32, A.tri, A.n_tri, n_rays, d_x, d_y, C,
+                                                   4 * A.n_tri + 64, d_rho, d_crossed, d_status,
+                                                   d_visits, max_record);
+    count_launch();
+  }
+  SDTFE_CUDA(cudaGetLastError());
+  return DTFE_OK;
 }
 
+}  // namespace sdtfe
+
+namespace sdtfe {
+int num_map32_variants() { return kNumVariants32; }
+void map32_variant_info(int i, int* block, int* minb, int* wide) {
+  *block = kVariants32[i].block;
+  *minb = kVariants32[i].minb;
+  *wide = kVariants32[i].wide;
+}
 }  // namespace sdtfe
