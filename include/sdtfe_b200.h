@@ -164,6 +164,24 @@ int dtfe_get_default_precision(void);
  * rand(), so that srand() keeps its meaning. */
 void dtfe_set_seed(uint64_t seed);
 
+/* Per-vertex DTFE density with no device allocation (no counterpart in the
+ * reference; it exists for callers that cannot allocate device memory mid-run:
+ * code inside a framework's memory pool or arena, serving loops that cannot
+ * afford the device-wide synchronisation of cudaMalloc/cudaFree, hosts that
+ * forbid allocation after start-up).  Inputs and output are device pointers
+ * in the reference layouts: d_particle_data (n*4 doubles, column 3 ignored),
+ * d_tetra_data (nt*8 ints); d_rho receives n densities, bit-identical to
+ * dtfe_mesh_density.  Temporaries live in one static 48 MiB device array held
+ * by every GPU that loads the library; sizes that do not fit (about 1.9M
+ * tets) are rejected with DTFE_ERR_UNSUPPORTED.  The first call on a device
+ * looks up that array's address (cudaGetSymbolAddress): make it before any
+ * stream capture.  All calls share the array, so calls that overlap on the
+ * GPU (other streams, other host threads) race; the call returns after its
+ * work on `stream` (NULL: the default stream) has finished. */
+dtfe_status_t dtfe_density_noalloc(const double *d_particle_data, int n_particles,
+                                   const int *d_tetra_data, int n_tetra, float p_mass,
+                                   double *d_rho, void *stream);
+
 /* Number of CUDA kernels this library has launched in this process (all
  * handles); benchmarks read it before and after a timed region. */
 unsigned long long dtfe_kernel_launches(void);
