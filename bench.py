@@ -236,13 +236,14 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def read_ncu_traffic(kernel, visits_per_launch):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, scaled
-    from the captured case to this launch by the number of tet visits."""
+def read_ncu_traffic(kernel, n_tets):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/traffic.json), scaled from the captured mesh to this one by the
+    tet count: the walk reads each tet record from DRAM about once per map."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         d = json.load(open(path))[kernel]
-        return d["dram_bytes"] / d["visits"] * visits_per_launch
+        return d["dram_bytes"] / d["tets"] * n_tets
     except (OSError, KeyError, ValueError, ZeroDivisionError):
         return None
 
@@ -399,7 +400,7 @@ def run_ours(args):
     peak_note = "measured" if peak else "fallback"
     peak = peak or 6650.0
     kname = "k_map32" if args.precision == "mixed" else "k_map64"
-    traffic = read_ncu_traffic(kname, visits)
+    traffic = read_ncu_traffic(kname, len(tetra))
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
