@@ -105,6 +105,7 @@ typedef struct {
 #define DTFE_MESH_NO_FP64_REC 2u /* keep no FP64 walk records (MIXED maps only)     */
 
 const char *dtfe_last_error(void);
+void dtfe_clear_error(void); /* empty the calling thread's last-error message */
 const char *dtfe_status_string(dtfe_status_t s);
 
 /* Upload a mesh and build everything the walks need.  Unless DTFE_MESH_FIELD is

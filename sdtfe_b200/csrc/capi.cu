@@ -108,6 +108,8 @@ extern "C" {
 
 const char* dtfe_last_error(void) { return t_err; }
 
+void dtfe_clear_error(void) { t_err[0] = '\0'; }
+
 const char* dtfe_status_string(dtfe_status_t s) {
   switch (s) {
     case DTFE_OK: return "ok";
