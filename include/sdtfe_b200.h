@@ -33,7 +33,8 @@ typedef enum {
   DTFE_ERR_MESH = 4,          /* index out of range in tetra_data               */
   DTFE_ERR_UNSUPPORTED = 5,   /* argument outside what this build implements   */
   DTFE_ERR_NO_TRIANGULATOR = 6, /* triangulate() called with no backend set     */
-  DTFE_ERR_ADMISSION = 7      /* request exceeds the serving memory budget      */
+  DTFE_ERR_ADMISSION = 7,     /* request exceeds the serving memory budget      */
+  DTFE_ERR_TIMEOUT = 8        /* dtfe_server_wait: the request is still running */
 } dtfe_status_t;
 
 /* arithmetic of the ray walk */
@@ -182,6 +183,98 @@ void dtfe_set_seed(uint64_t seed);
 dtfe_status_t dtfe_density_noalloc(const double *d_particle_data, int n_particles,
                                    const int *d_tetra_data, int n_tetra, float p_mass,
                                    double *d_rho, void *stream);
+
+/* ---- Batched maps -----------------------------------------------------
+ * Maps of many meshes (cutouts) in one persistent kernel launch: the blocks
+ * pull pixel tiles of every map from one device counter, so maps of uneven
+ * size share the GPU with no tail per map.  Each map's result is
+ * bit-identical to dtfe_map_device with the same parameters.  No counterpart
+ * in the reference, which maps one mesh per call (src/dtfe.c:554-654). */
+typedef struct {
+  dtfe_mesh_t mesh;
+  dtfe_map_params_t params;  /* every job of a batch has the same precision    */
+  double *d_map;             /* grid_dim^2 doubles on the device, accumulated  */
+} dtfe_batch_job_t;
+
+typedef struct dtfe_batch_s *dtfe_batch_t;
+
+#define DTFE_BATCH_GRAPH 1u     /* capture the launch once in a CUDA graph and replay it */
+#define DTFE_BATCH_ZERO_MAPS 2u /* zero every map before each launch                  */
+
+/* Builds every job's records and hull (on the meshes' streams), plans the
+ * tile queue and uploads the job table.  The meshes and maps must outlive
+ * the batch, and the meshes take no other calls while its launches run. */
+dtfe_status_t dtfe_batch_create(const dtfe_batch_job_t *jobs, int n_jobs, unsigned flags,
+                                dtfe_batch_t *out);
+/* One launch over all jobs, asynchronous on `stream` (NULL: the batch's own). */
+dtfe_status_t dtfe_batch_launch(dtfe_batch_t batch, void *stream);
+dtfe_status_t dtfe_batch_sync(dtfe_batch_t batch);
+/* Counters of the last launch, per job (walk_ms: the whole launch). */
+dtfe_status_t dtfe_batch_stats(dtfe_batch_t batch, dtfe_map_stats_t *per_job);
+/* Mixed batches: time every kernel variant over the whole batch (maps are
+ * zeroed afterwards) and keep the fastest. */
+dtfe_status_t dtfe_batch_autotune(dtfe_batch_t batch, int *best, dtfe_variant_t *timings);
+dtfe_status_t dtfe_batch_set_variant(dtfe_batch_t batch, int variant);
+/* persistent grid: blocks, threads per block, tiles in the queue */
+dtfe_status_t dtfe_batch_info(dtfe_batch_t batch, int *grid, int *block, long long *tiles);
+dtfe_status_t dtfe_batch_destroy(dtfe_batch_t batch);
+
+/* ---- Serving loop ------------------------------------------------------
+ * A host thread that keeps many meshes resident and serves map requests as
+ * they arrive, with continuous batching: every iteration is one persistent
+ * launch over a slice of the tiles of every admitted request, so requests
+ * that arrive while others run join the next iteration, and consecutive
+ * iterations overlap on two streams.  Requests are admitted while a slot is
+ * free and their map buffer plus any walk records they need fit the device
+ * budget; records of idle (mesh, axis) pairs are evicted least recently used
+ * first.  A request's map is the same alone and in any mix: every pixel is
+ * formed by one block from its own samples, whatever else the launch holds. */
+typedef struct dtfe_server_s *dtfe_server_t;
+
+#define DTFE_SERVE_FAIR 0  /* each iteration splits its tiles evenly over requests */
+#define DTFE_SERVE_FIFO 1  /* each iteration serves the oldest requests first      */
+
+typedef struct {
+  size_t device_budget;    /* bytes for walk records and maps (0: 3/4 of free memory) */
+  int max_active;          /* requests on the GPU at once (0: 64)                     */
+  long long quantum_rays;  /* rays per iteration launch (0: 2^20)                     */
+  int policy;              /* DTFE_SERVE_FAIR or DTFE_SERVE_FIFO                      */
+  int variant;             /* mixed kernel variant (-1: default)                      */
+} dtfe_server_config_t;
+
+typedef struct {
+  int status;              /* dtfe_status_t of the request                            */
+  double queue_ms;         /* submit -> admitted                                      */
+  double latency_ms;       /* submit -> map in the caller's buffer                    */
+  int iterations;          /* launches that walked some of its tiles                  */
+  dtfe_map_stats_t stats;  /* its rays, visits, statuses (walk_ms: 0)                 */
+} dtfe_request_info_t;
+
+typedef struct {
+  unsigned long long submitted, completed, failed;
+  unsigned long long iterations;     /* kernel launches of the loop                  */
+  unsigned long long rays, visits;   /* of completed requests                        */
+  unsigned long long evictions;      /* walk records dropped for memory              */
+  size_t budget, in_use, peak;       /* device bytes under the budget                */
+  int active, queued;                /* right now                                    */
+} dtfe_server_stats_t;
+
+dtfe_status_t dtfe_server_create(const dtfe_server_config_t *cfg, dtfe_server_t *out);
+/* Registers a mesh (the caller keeps it; it must outlive the server and take
+ * no other calls while registered).  Its current walk records count against
+ * the budget and may be evicted. */
+dtfe_status_t dtfe_server_add_mesh(dtfe_server_t server, dtfe_mesh_t mesh, int *mesh_id);
+/* Queues one map of mesh `mesh_id`; the map (grid_dim^2 doubles, host
+ * memory, overwritten) is written when the request completes. */
+dtfe_status_t dtfe_server_submit(dtfe_server_t server, int mesh_id, const dtfe_map_params_t *p,
+                                 double *map, uint64_t *request_id);
+/* Waits up to timeout_ms (< 0: forever) for a request; DTFE_ERR_TIMEOUT if it
+ * is still running.  A completed request's info can be read once. */
+dtfe_status_t dtfe_server_wait(dtfe_server_t server, uint64_t request_id, int timeout_ms,
+                               dtfe_request_info_t *info);
+dtfe_status_t dtfe_server_stats(dtfe_server_t server, dtfe_server_stats_t *stats);
+/* Finishes every queued request, then stops the loop and frees its memory. */
+dtfe_status_t dtfe_server_destroy(dtfe_server_t server);
 
 /* Number of CUDA kernels this library has launched in this process (all
  * handles); benchmarks read it before and after a timed region. */

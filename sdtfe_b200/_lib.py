@@ -70,6 +70,52 @@ class Variant(ctypes.Structure):
     _fields_ = [("block", _i), ("min_blocks", _i), ("wide_tile", _i), ("ms", _d)]
 
 
+class BatchJob(ctypes.Structure):
+    _fields_ = [("mesh", _vp), ("params", MapParams), ("d_map", _vp)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device_budget", ctypes.c_size_t),
+        ("max_active", _i),
+        ("quantum_rays", ctypes.c_longlong),
+        ("policy", _i),
+        ("variant", _i),
+    ]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("status", _i),
+        ("queue_ms", _d),
+        ("latency_ms", _d),
+        ("iterations", _i),
+        ("stats", MapStats),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_ulonglong),
+        ("completed", ctypes.c_ulonglong),
+        ("failed", ctypes.c_ulonglong),
+        ("iterations", ctypes.c_ulonglong),
+        ("rays", ctypes.c_ulonglong),
+        ("visits", ctypes.c_ulonglong),
+        ("evictions", ctypes.c_ulonglong),
+        ("budget", ctypes.c_size_t),
+        ("in_use", ctypes.c_size_t),
+        ("peak", ctypes.c_size_t),
+        ("active", _i),
+        ("queued", _i),
+    ]
+
+
+BATCH_GRAPH, BATCH_ZERO_MAPS = 1, 2
+SERVE_FAIR, SERVE_FIFO = 0, 1
+ERR_ADMISSION, ERR_TIMEOUT = 7, 8
+
+
 class DTFEError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"status {status}: {msg}")
@@ -112,6 +158,23 @@ def lib() -> ctypes.CDLL:
     L.dtfe_autotune.argtypes = [_vp, ctypes.POINTER(MapParams), ctypes.POINTER(_i), _vp]
     L.dtfe_set_variant.argtypes = [_vp, _i]
     L.dtfe_tetra_from_cells.argtypes = [_f64, _i32, _i32, ctypes.c_size_t, _i32]
+    # batches and the serving loop
+    L.dtfe_batch_create.argtypes = [ctypes.POINTER(BatchJob), _i, ctypes.c_uint, ctypes.POINTER(_vp)]
+    L.dtfe_batch_launch.argtypes = [_vp, _vp]
+    L.dtfe_batch_sync.argtypes = [_vp]
+    L.dtfe_batch_stats.argtypes = [_vp, ctypes.POINTER(MapStats)]
+    L.dtfe_batch_autotune.argtypes = [_vp, ctypes.POINTER(_i), _vp]
+    L.dtfe_batch_set_variant.argtypes = [_vp, _i]
+    L.dtfe_batch_info.argtypes = [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i),
+                                  ctypes.POINTER(ctypes.c_longlong)]
+    L.dtfe_batch_destroy.argtypes = [_vp]
+    L.dtfe_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]
+    L.dtfe_server_add_mesh.argtypes = [_vp, _vp, ctypes.POINTER(_i)]
+    L.dtfe_server_submit.argtypes = [_vp, _i, ctypes.POINTER(MapParams), _vp,
+                                     ctypes.POINTER(ctypes.c_uint64)]
+    L.dtfe_server_wait.argtypes = [_vp, ctypes.c_uint64, _i, ctypes.POINTER(RequestInfo)]
+    L.dtfe_server_stats.argtypes = [_vp, ctypes.POINTER(ServerStats)]
+    L.dtfe_server_destroy.argtypes = [_vp]
     # drop-ins
     L.compute_density.argtypes = [_f64, _i, _i32, _i, _i, _d, _d, _f64, ctypes.c_float, _d, _d,
                                   _d, _i, _d]
@@ -279,3 +342,120 @@ class Mesh:
         c = (_d * 3)(*center)
         _check(lib().dtfe_grid(self.h, G, box_len, c, ss, seed, g.reshape(-1)))
         return g
+
+
+class Batch:
+    """Maps of several meshes in one persistent launch (dtfe_batch_t).
+
+    jobs: list of (Mesh, MapParams, device pointer of a grid_dim^2 float64 map)."""
+
+    def __init__(self, jobs, flags: int = 0):
+        self.meshes = [j[0] for j in jobs]  # keep the meshes alive
+        arr = (BatchJob * len(jobs))()
+        for k, (mesh, params, d_map) in enumerate(jobs):
+            arr[k].mesh = mesh.h
+            arr[k].params = params
+            arr[k].d_map = d_map
+        self.n = len(jobs)
+        h = _vp()
+        _check(lib().dtfe_batch_create(arr, len(jobs), flags, ctypes.byref(h)))
+        self.h = h
+
+    def launch(self, stream_ptr: int = 0):
+        _check(lib().dtfe_batch_launch(self.h, _vp(stream_ptr) if stream_ptr else None))
+
+    def sync(self):
+        _check(lib().dtfe_batch_sync(self.h))
+
+    def stats(self):
+        arr = (MapStats * self.n)()
+        _check(lib().dtfe_batch_stats(self.h, arr))
+        return list(arr)
+
+    def autotune(self):
+        n = lib().dtfe_num_variants()
+        arr = (Variant * n)()
+        best = _i()
+        _check(lib().dtfe_batch_autotune(self.h, ctypes.byref(best), arr))
+        return best.value, [dict(block=v.block, min_blocks=v.min_blocks, wide_tile=v.wide_tile,
+                                 ms=v.ms) for v in arr]
+
+    def set_variant(self, v: int):
+        _check(lib().dtfe_batch_set_variant(self.h, v))
+
+    def info(self):
+        g, b, t = _i(), _i(), ctypes.c_longlong()
+        _check(lib().dtfe_batch_info(self.h, ctypes.byref(g), ctypes.byref(b), ctypes.byref(t)))
+        return dict(grid=g.value, block=b.value, tiles=t.value)
+
+    def close(self):
+        if self.h:
+            lib().dtfe_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving loop (dtfe_server_t): submit map requests, wait for them."""
+
+    def __init__(self, device_budget: int = 0, max_active: int = 0, quantum_rays: int = 0,
+                 policy: int = SERVE_FAIR, variant: int = -1):
+        c = ServerConfig(device_budget, max_active, quantum_rays, policy, variant)
+        h = _vp()
+        _check(lib().dtfe_server_create(ctypes.byref(c), ctypes.byref(h)))
+        self.h = h
+        self.meshes = []
+        self._maps = {}
+
+    def add_mesh(self, mesh: Mesh) -> int:
+        i = _i()
+        _check(lib().dtfe_server_add_mesh(self.h, mesh.h, ctypes.byref(i)))
+        self.meshes.append(mesh)
+        return i.value
+
+    def submit(self, mesh_id: int, params: MapParams, out: np.ndarray | None = None) -> int:
+        G = params.grid_dim
+        m = np.empty((G, G), np.float64) if out is None else out
+        assert m.flags.c_contiguous and m.dtype == np.float64 and m.size == G * G
+        rid = ctypes.c_uint64()
+        _check(lib().dtfe_server_submit(self.h, mesh_id, ctypes.byref(params),
+                                        m.ctypes.data_as(_vp), ctypes.byref(rid)))
+        self._maps[rid.value] = m
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1):
+        """(map, RequestInfo) of a finished request; raises DTFEError on failure or timeout."""
+        info = RequestInfo()
+        st = lib().dtfe_server_wait(self.h, rid, timeout_ms, ctypes.byref(info))
+        if st == ERR_TIMEOUT:
+            raise DTFEError(st, lib().dtfe_last_error().decode())
+        m = self._maps.pop(rid, None)
+        _check(st)
+        return m, info
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        _check(lib().dtfe_server_stats(self.h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if self.h:
+            lib().dtfe_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

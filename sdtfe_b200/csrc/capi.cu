@@ -13,11 +13,6 @@
 #include "mesh.h"
 #include "triangulate.h"
 
-struct dtfe_mesh_s {
-  sdtfe::Mesh m;
-  std::mutex mu;  // one call at a time per handle
-};
-
 namespace sdtfe {
 
 static thread_local char t_err[512] = "";
@@ -36,14 +31,7 @@ void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxe
 
 }  // namespace sdtfe
 
-using namespace sdtfe;
-
-namespace {
-
-int g_default_precision = -1;  // -1: read SDTFE_PRECISION once
-uint64_t g_seed = 0;
-dtfe_triangulator_fn g_tri_fn = nullptr;
-void* g_tri_user = nullptr;
+namespace sdtfe {
 
 dtfe_status_t check_params(const Mesh& m, const dtfe_map_params_t* p) {
   if (!p) return set_error(DTFE_ERR_INVALID, "params is NULL");
@@ -68,10 +56,21 @@ dtfe_status_t prepare_axis(Mesh& m, int axis, int precision) {
   if (!m.grad) SDTFE_TRY(mesh_gradients(&m));
   const bool want64 = precision == DTFE_FP64 || !(m.flags & DTFE_MESH_NO_FP64_REC);
   const bool want32 = precision == DTFE_MIXED;
-  SDTFE_TRY(mesh_records(&m, axis, want64, want32 || m.rec32 != nullptr));
+  SDTFE_TRY(mesh_records(&m, axis, want64, want32));
   SDTFE_TRY(mesh_hull(&m, axis, nullptr, nullptr));
   return DTFE_OK;
 }
+
+}  // namespace sdtfe
+
+using namespace sdtfe;
+
+namespace {
+
+int g_default_precision = -1;  // -1: read SDTFE_PRECISION once
+uint64_t g_seed = 0;
+dtfe_triangulator_fn g_tri_fn = nullptr;
+void* g_tri_user = nullptr;
 
 dtfe_status_t launch_map(Mesh& m, const dtfe_map_params_t* p, double* d_map, cudaStream_t s,
                          double* rr = nullptr, int* rc = nullptr, int* rs = nullptr) {
@@ -120,6 +119,7 @@ const char* dtfe_status_string(dtfe_status_t s) {
     case DTFE_ERR_UNSUPPORTED: return "unsupported";
     case DTFE_ERR_NO_TRIANGULATOR: return "no triangulator registered";
     case DTFE_ERR_ADMISSION: return "admission refused";
+    case DTFE_ERR_TIMEOUT: return "timed out";
   }
   return "unknown";
 }
@@ -244,8 +244,10 @@ dtfe_status_t dtfe_map_device(dtfe_mesh_t h, const dtfe_map_params_t* p, double*
   std::lock_guard<std::mutex> lk(h->mu);
   Mesh& m = h->m;
   SDTFE_TRY(check_params(m, p));
-  const bool ready = m.rec_axis == p->axis && m.ax[p->axis].hull_built &&
-                     (p->precision == DTFE_FP64 ? m.rec64 != nullptr : m.rec32 != nullptr);
+  const AxisData& A = m.ax[p->axis];
+  const bool ready = A.hull_built && (p->precision == DTFE_FP64 ? A.rec64 != nullptr
+                                                                 : A.rec32 != nullptr &&
+                                                                       (m.fp32_exact || A.rec64));
   cudaStream_t s = stream ? (cudaStream_t)stream : m.stream;
   if (!ready) {
     SDTFE_TRY(prepare_axis(m, p->axis, p->precision));
@@ -372,9 +374,9 @@ dtfe_status_t dtfe_trace(dtfe_mesh_t h, const dtfe_map_params_t* p, int n_rays, 
   SDTFE_CUDA(cudaMemcpyAsync(dy, y, sizeof(double) * n_rays, cudaMemcpyHostToDevice, s));
   dtfe_status_t st =
       p->precision == DTFE_MIXED
-          ? launch_trace32(m, n_rays, dx, dy, z0, lz, delta_xy, p->seed, max_visits, dr, dc, ds, dv,
+          ? launch_trace32(m, p->axis, n_rays, dx, dy, z0, lz, delta_xy, p->seed, max_visits, dr, dc, ds, dv,
                            max_record, s)
-          : launch_trace64(m, n_rays, dx, dy, z0, lz, delta_xy, p->seed, max_visits, dr, dc, ds, dv,
+          : launch_trace64(m, p->axis, n_rays, dx, dy, z0, lz, delta_xy, p->seed, max_visits, dr, dc, ds, dv,
                            max_record, s);
   if (st == DTFE_OK) {
     cudaError_t e = cudaMemcpyAsync(rho, dr, sizeof(double) * n_rays, cudaMemcpyDeviceToHost, s);

@@ -435,18 +435,27 @@ dtfe_status_t mesh_gradients(Mesh* m) {
 dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32) {
   if (axis < 0 || axis > 2) return set_error(DTFE_ERR_INVALID, "axis %d not in 0..2", axis);
   if (!m->grad) return set_error(DTFE_ERR_INVALID, "mesh_records before mesh_gradients");
-  const bool have64 = m->rec64 != nullptr, have32 = m->rec32 != nullptr;
-  if (m->rec_axis == axis && (!want64 || have64) && (!want32 || have32)) return DTFE_OK;
-  if (want64 && !m->rec64) SDTFE_TRY(dmalloc(&m->rec64, m->nt, m));
-  if (want32 && !m->rec32) SDTFE_TRY(dmalloc(&m->rec32, m->nt, m));
+  AxisData& A = m->ax[axis];
+  const bool need64 = want64 && !A.rec64, need32 = want32 && !A.rec32;
+  if (!need64 && !need32) return DTFE_OK;
+  if (need64) SDTFE_TRY(dmalloc(&A.rec64, m->nt, m));
+  if (need32) SDTFE_TRY(dmalloc(&A.rec32, m->nt, m));
   if (m->nt) {
     k_records<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, axis,
-                                                         m->rec64, m->rec32);
+                                                         need64 ? A.rec64 : nullptr,
+                                                         need32 ? A.rec32 : nullptr);
     count_launch();
   }
   SDTFE_CUDA(cudaGetLastError());
-  m->rec_axis = axis;
   return DTFE_OK;
+}
+
+// Frees one axis' walk records (the caller has no map of that axis in flight).
+void mesh_drop_records(Mesh* m, int axis) {
+  if (axis < 0 || axis > 2) return;
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  dfree(m->ax[axis].rec64, m->nt, m);
+  dfree(m->ax[axis].rec32, m->nt, m);
 }
 
 dtfe_status_t mesh_hull_mask(Mesh* m, int axis, uint32_t* host_mask_out, int* count_out) {
@@ -557,10 +566,10 @@ void mesh_free(Mesh* m) {
   dfree(m->rows, 2 * (size_t)m->nt, m);
   dfree(m->grad, 3 * (size_t)m->nt, m);
   dfree(m->adj, m->n, m);
-  dfree(m->rec64, m->nt, m);
-  dfree(m->rec32, m->nt, m);
   dfree(m->stats, kStatCount, m);
   for (auto& A : m->ax) {
+    dfree(A.rec64, m->nt, m);
+    dfree(A.rec32, m->nt, m);
     dfree(A.tri, A.n_tri, m);
     dfree(A.tri_rows, 8 * (size_t)A.n_tri, m);
   }

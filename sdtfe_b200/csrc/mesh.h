@@ -5,7 +5,9 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "sdtfe_b200.h"
 #include "walk64.cuh"
@@ -49,6 +51,9 @@ struct AxisData {
   int n_tri = 0;
   TriRec64* tri = nullptr;  // device, n_tri records
   int* tri_rows = nullptr;  // device, n_tri * 8 ints in the reference's tri_data layout
+  // walk records in this axis' projected frame (built on demand, per precision)
+  TetRec64* rec64 = nullptr;
+  TetRec32* rec32 = nullptr;
 };
 
 struct Mesh {
@@ -63,9 +68,6 @@ struct Mesh {
   int4* rows = nullptr;     // 2 per tet: vertex ids, neighbour ids
   double* grad = nullptr;   // 3 per tet
   int* adj = nullptr;       // tets incident to each vertex
-  int rec_axis = -1;        // axis the walk records are built for
-  TetRec64* rec64 = nullptr;
-  TetRec32* rec32 = nullptr;
   AxisData ax[3];
   unsigned long long* stats = nullptr;  // kStatCount counters of the last map
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -80,6 +82,7 @@ dtfe_status_t mesh_upload(Mesh* m, const double* particle_data, int n, const int
 dtfe_status_t mesh_density(Mesh* m);
 dtfe_status_t mesh_gradients(Mesh* m);
 dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32);
+void mesh_drop_records(Mesh* m, int axis);
 // host_mask (optional) replaces the forward-face test with a caller's bitmap
 // (one 32-bit word per tet, faces in bits 0..3)
 dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count_out);
@@ -98,8 +101,14 @@ __host__ __device__ inline void permute3(int axis, double x, double y, double z,
   }
 }
 
+// capi.cu: parameter checks, and the records + hull a map of (axis,
+// precision) reads, built on the mesh stream
+dtfe_status_t check_params(const Mesh& m, const dtfe_map_params_t* p);
+dtfe_status_t prepare_axis(Mesh& m, int axis, int precision);
+
 // walk.cu / walk32.cu launchers
 struct MapGeom {
+  int axis;
   int G, S;
   double dxy, offx, offy, offz, lz, scale, soff, dist;
   uint64_t seed;
@@ -110,17 +119,57 @@ dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
                            double* ray_rho, int* ray_crossed, int* ray_status);
 dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
                            double* ray_rho, int* ray_crossed, int* ray_status);
-dtfe_status_t launch_trace64(Mesh& m, int n_rays, const double* d_x, const double* d_y, double z0,
-                             double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
-                             int* d_crossed, int* d_status, int* d_visits, int max_record,
-                             cudaStream_t s);
-dtfe_status_t launch_trace32(Mesh& m, int n_rays, const double* d_x, const double* d_y, double z0,
-                             double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
-                             int* d_crossed, int* d_status, int* d_visits, int max_record,
-                             cudaStream_t s);
+dtfe_status_t launch_trace64(Mesh& m, int axis, int n_rays, const double* d_x, const double* d_y,
+                             double z0, double lz, double dxy, uint64_t seed, int max_visits,
+                             double* d_rho, int* d_crossed, int* d_status, int* d_visits,
+                             int max_record, cudaStream_t s);
+dtfe_status_t launch_trace32(Mesh& m, int axis, int n_rays, const double* d_x, const double* d_y,
+                             double z0, double lz, double dxy, uint64_t seed, int max_visits,
+                             double* d_rho, int* d_crossed, int* d_status, int* d_visits,
+                             int max_record, cudaStream_t s);
 int num_map32_variants();
 void map32_variant_info(int i, int* block, int* minb, int* wide);
 dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
                             uint64_t seed, int max_visits, double* d_grid, cudaStream_t s);
 
+// Batched maps (walk.cu, walk32.cu): one persistent launch walks the tiles of
+// several maps, pulled from a device counter.  A map may be split into ranges
+// of tiles that go to different launches (the serving loop does that).
+struct BatchMap {
+  Mesh* mesh;
+  MapGeom g;
+  double* d_map;              // the map, accumulated
+  unsigned long long* stats;  // kStatCount device counters for this map
+  int tile0 = 0;              // the range of the map's tiles this launch walks
+  int count = -1;             // (-1: from tile0 to the end)
+};
+struct BatchPlan {
+  int precision = DTFE_FP64;
+  int variant = -1;           // mixed kernel variant (ignored for FP64)
+  int n_jobs = 0;
+  long long total_tiles = 0;
+  size_t smem = 0;            // dynamic shared memory per block
+  std::vector<unsigned char> jobs;  // the job table as the kernel reads it
+};
+// tiles of a whole map (the tile shape depends on precision and variant)
+int map_tiles64(const MapGeom& g);
+int map_tiles32(const MapGeom& g, int variant);
+dtfe_status_t plan_batch64(const BatchMap* maps, int n, BatchPlan* plan);
+dtfe_status_t plan_batch32(const BatchMap* maps, int n, int variant, BatchPlan* plan);
+// blocks of a persistent launch: resident blocks per SM x SMs
+dtfe_status_t batch_grid64(size_t smem, int* grid, int* block);
+dtfe_status_t batch_grid32(int variant, size_t smem, int* grid, int* block);
+// d_jobs holds plan.jobs; d_queue is a zeroed counter
+dtfe_status_t launch_batch64(const BatchPlan& plan, const void* d_jobs, unsigned long long* d_queue,
+                             int grid, cudaStream_t s);
+dtfe_status_t launch_batch32(const BatchPlan& plan, const void* d_jobs, unsigned long long* d_queue,
+                             int grid, cudaStream_t s);
+int default_variant32();
+
 }  // namespace sdtfe
+
+// the object behind a dtfe_mesh_t handle
+struct dtfe_mesh_s {
+  sdtfe::Mesh m;
+  std::mutex mu;  // one call at a time per handle
+};

@@ -10,6 +10,7 @@
 // sample order and divides by the successful count, which reproduces the
 // reference's per-pixel sum order (src/dtfe.c:615-645).
 #include <cstdio>
+#include <cstring>
 
 #include "mesh.h"
 
@@ -30,6 +31,13 @@ struct MapArgs64 {
   double* __restrict__ ray_rho;
   int* __restrict__ ray_crossed;
   int* __restrict__ ray_status;
+};
+
+struct BatchJob64 {
+  MapArgs64 args;
+  long long first;  // first global tile of the job
+  int tile0;        // the job's first tile within its map
+  int count;
 };
 
 // warp-aggregated counters: one atomic per warp and counter
@@ -54,13 +62,11 @@ __device__ __forceinline__ void add_stats(unsigned long long* stats, bool active
   }
 }
 
-__global__ void __launch_bounds__(256) k_map64(const MapArgs64 a) {
-  extern __shared__ double s_val[];  // P*S doubles, then P*S bytes of success flags
+// One tile of one map (TW x TH pixels x S samples) on the block's threads.
+__device__ __forceinline__ void map_tile64(const MapArgs64& a, int tile, double* s_val,
+                                           unsigned char* s_ok) {
   const int P = a.TW * a.TH;
-  unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val + P * a.S);
-  const int tile = blockIdx.x;
   const int tx0 = (tile % a.tiles_x) * a.TW, ty0 = (tile / a.tiles_x) * a.TH;
-
   for (int t = threadIdx.x; t < P * a.S; t += blockDim.x) {
     const int lp = t / a.S, s = t % a.S;
     const int col = tx0 + lp % a.TW, row = ty0 + lp / a.TW;
@@ -102,6 +108,50 @@ __global__ void __launch_bounds__(256) k_map64(const MapArgs64 a) {
       n_avg += s_ok[lp * a.S + s];
     }
     a.map[(size_t)row * a.G + col] += n_avg > 0 ? total / n_avg : 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_map64(const MapArgs64 a) {
+  extern __shared__ double s_val[];  // P*S doubles, then P*S bytes of success flags
+  unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val + a.TW * a.TH * a.S);
+  map_tile64(a, blockIdx.x, s_val, s_ok);
+}
+
+// Persistent batch over several maps (see k_batch32 in walk32.cu).
+__global__ void __launch_bounds__(256) k_batch64(const BatchJob64* __restrict__ jobs, int n_jobs,
+                                                 long long total_tiles,
+                                                 unsigned long long* __restrict__ queue) {
+  extern __shared__ double s_val[];
+  __shared__ MapArgs64 s_args;
+  __shared__ long long s_tile;
+  __shared__ int s_job;
+  int cur_job = -1;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_tile = (long long)atomicAdd(queue, 1ull);
+      int lo = 0, hi = n_jobs - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (jobs[mid].first <= s_tile) lo = mid;
+        else hi = mid - 1;
+      }
+      s_job = lo;
+    }
+    __syncthreads();
+    const long long tile = s_tile;
+    const int j = s_job;
+    if (tile >= total_tiles) break;
+    if (j != cur_job) {
+      const int* src = reinterpret_cast<const int*>(&jobs[j].args);
+      int* dst = reinterpret_cast<int*>(&s_args);
+      for (int k = threadIdx.x; k < (int)(sizeof(MapArgs64) / sizeof(int)); k += blockDim.x)
+        dst[k] = src[k];
+      cur_job = j;
+    }
+    __syncthreads();
+    unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val + s_args.TW * s_args.TH * s_args.S);
+    map_tile64(s_args, jobs[j].tile0 + (int)(tile - jobs[j].first), s_val, s_ok);
+    __syncthreads();
   }
 }
 
@@ -173,6 +223,7 @@ __global__ void __launch_bounds__(128) k_grid64(const TetRec64* __restrict__ rec
 
 MapGeom map_geometry(const Mesh& m, const dtfe_map_params_t& p) {
   MapGeom g;
+  g.axis = p.axis;
   g.G = p.grid_dim;
   g.S = p.n_samples;
   // src/dtfe.c:579-589, in the projected frame
@@ -205,11 +256,14 @@ static void tile_shape(int S, int* TW, int* TH) {
   *TH = th;
 }
 
-dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
-                           double* ray_rho, int* ray_crossed, int* ray_status) {
-  const AxisData& A = m.ax[m.rec_axis];
-  MapArgs64 a;
-  a.rec = m.rec64;
+// The kernel arguments of one FP64 map; *tiles_y receives its rows of tiles.
+static dtfe_status_t map_args64(Mesh& m, const MapGeom& g, double* d_map,
+                                unsigned long long* stats, double* ray_rho, int* ray_crossed,
+                                int* ray_status, MapArgs64* out, int* tiles_y) {
+  const AxisData& A = m.ax[g.axis];
+  if (!A.rec64 || !A.hull_built) return set_error(DTFE_ERR_INVALID, "FP64 map before its records");
+  MapArgs64& a = *out;
+  a.rec = A.rec64;
   a.tri = A.tri;
   a.n_tri = A.n_tri;
   a.map = d_map;
@@ -217,7 +271,7 @@ dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   a.S = g.S;
   tile_shape(g.S, &a.TW, &a.TH);
   a.tiles_x = (g.G + a.TW - 1) / a.TW;
-  const int tiles_y = (g.G + a.TH - 1) / a.TH;
+  *tiles_y = (g.G + a.TH - 1) / a.TH;
   a.dxy = g.dxy;
   a.offx = g.offx;
   a.offy = g.offy;
@@ -227,10 +281,18 @@ dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   a.soff = g.soff;
   a.walk = WalkConf64{g.lz, g.dist, g.seed, g.max_visits};
   a.loc_budget = 4 * A.n_tri + 64;
-  a.stats = m.stats;
+  a.stats = stats;
   a.ray_rho = ray_rho;
   a.ray_crossed = ray_crossed;
   a.ray_status = ray_status;
+  return DTFE_OK;
+}
+
+dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
+                           double* ray_rho, int* ray_crossed, int* ray_status) {
+  MapArgs64 a;
+  int tiles_y = 0;
+  SDTFE_TRY(map_args64(m, g, d_map, m.stats, ray_rho, ray_crossed, ray_status, &a, &tiles_y));
   const int P = a.TW * a.TH;
   int threads = P * g.S;
   threads = threads > 256 ? 256 : ((threads + 31) / 32) * 32;
@@ -248,14 +310,77 @@ dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   return DTFE_OK;
 }
 
-dtfe_status_t launch_trace64(Mesh& m, int n_rays, const double* d_x, const double* d_y, double z0,
-                             double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
-                             int* d_crossed, int* d_status, int* d_visits, int max_record,
-                             cudaStream_t s) {
-  const AxisData& A = m.ax[m.rec_axis];
+int map_tiles64(const MapGeom& g) {
+  int TW, TH;
+  tile_shape(g.S, &TW, &TH);
+  return ((g.G + TW - 1) / TW) * ((g.G + TH - 1) / TH);
+}
+
+dtfe_status_t plan_batch64(const BatchMap* maps, int n, BatchPlan* plan) {
+  plan->precision = DTFE_FP64;
+  plan->variant = -1;
+  plan->n_jobs = 0;
+  plan->total_tiles = 0;
+  plan->smem = 0;
+  plan->jobs.assign(sizeof(BatchJob64) * (size_t)(n > 0 ? n : 0), 0);
+  for (int i = 0; i < n; ++i) {
+    const BatchMap& b = maps[i];
+    BatchJob64 j;
+    int tiles_y = 0;
+    SDTFE_TRY(map_args64(*b.mesh, b.g, b.d_map, b.stats, nullptr, nullptr, nullptr, &j.args, &tiles_y));
+    const long long tiles = (long long)j.args.tiles_x * tiles_y;
+    const long long cnt = b.count < 0 ? tiles - b.tile0 : b.count;
+    if (b.tile0 < 0 || cnt < 0 || b.tile0 + cnt > tiles)
+      return set_error(DTFE_ERR_INVALID, "batch map %d: tiles [%d, %lld) outside the map's %lld", i,
+                       b.tile0, b.tile0 + cnt, tiles);
+    if (cnt == 0) continue;
+    j.first = plan->total_tiles;
+    j.tile0 = b.tile0;
+    j.count = (int)cnt;
+    memcpy(plan->jobs.data() + sizeof(BatchJob64) * plan->n_jobs, &j, sizeof(j));
+    ++plan->n_jobs;
+    plan->total_tiles += cnt;
+    const size_t smem = (size_t)j.args.TW * j.args.TH * j.args.S * (sizeof(double) + 1);
+    if (smem > plan->smem) plan->smem = smem;
+  }
+  plan->jobs.resize(sizeof(BatchJob64) * plan->n_jobs);
+  return DTFE_OK;
+}
+
+dtfe_status_t batch_grid64(size_t smem, int* grid, int* block) {
+  int dev = 0, sms = 0, per_sm = 0;
+  SDTFE_CUDA(cudaGetDevice(&dev));
+  SDTFE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (smem > 48 * 1024)
+    SDTFE_CUDA(cudaFuncSetAttribute(k_batch64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SDTFE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch64, 256, smem));
+  if (per_sm < 1) return set_error(DTFE_ERR_UNSUPPORTED, "FP64 batch: %zu B of shared memory per block", smem);
+  *grid = per_sm * sms;
+  *block = 256;
+  return DTFE_OK;
+}
+
+dtfe_status_t launch_batch64(const BatchPlan& plan, const void* d_jobs, unsigned long long* d_queue,
+                             int grid, cudaStream_t s) {
+  if (plan.n_jobs == 0) return DTFE_OK;
+  if (plan.smem > 48 * 1024)
+    SDTFE_CUDA(cudaFuncSetAttribute(k_batch64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem));
+  k_batch64<<<grid, 256, plan.smem, s>>>(static_cast<const BatchJob64*>(d_jobs), plan.n_jobs,
+                                         plan.total_tiles, d_queue);
+  count_launch();
+  SDTFE_CUDA(cudaGetLastError());
+  return DTFE_OK;
+}
+
+dtfe_status_t launch_trace64(Mesh& m, int axis, int n_rays, const double* d_x, const double* d_y,
+                             double z0, double lz, double dxy, uint64_t seed, int max_visits,
+                             double* d_rho, int* d_crossed, int* d_status, int* d_visits,
+                             int max_record, cudaStream_t s) {
+  const AxisData& A = m.ax[axis];
+  if (!A.rec64 || !A.hull_built) return set_error(DTFE_ERR_INVALID, "FP64 trace before its records");
   WalkConf64 w{lz, (dxy / 2.0) / kPerturbMax, seed, max_visits};
   if (n_rays > 0) {
-    k_trace64<<<(n_rays + 127) / 128, 128, 0, s>>>(m.rec64, A.tri, A.n_tri, n_rays, d_x, d_y, z0, w,
+    k_trace64<<<(n_rays + 127) / 128, 128, 0, s>>>(A.rec64, A.tri, A.n_tri, n_rays, d_x, d_y, z0, w,
                                                    4 * A.n_tri + 64, d_rho, d_crossed, d_status,
                                                    d_visits, max_record);
     count_launch();
@@ -266,7 +391,8 @@ dtfe_status_t launch_trace64(Mesh& m, int n_rays, const double* d_x, const doubl
 
 dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
                             uint64_t seed, int max_visits, double* d_grid, cudaStream_t s) {
-  const AxisData& A = m.ax[m.rec_axis];
+  const AxisData& A = m.ax[DTFE_AXIS_Z];
+  if (!A.rec64 || !A.hull_built) return set_error(DTFE_ERR_INVALID, "grid before its records");
   const double dxy = box_len / G;
   const double offx = -(box_len / 2.0) + center[0];
   const double offy = -(box_len / 2.0) + center[1];
@@ -275,7 +401,7 @@ dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[
   const long long ncol = (long long)G * G;
   SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
   SDTFE_CUDA(cudaEventRecord(m.ev0, s));
-  k_grid64<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(m.rec64, A.tri, A.n_tri, G, dxy, offx,
+  k_grid64<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(A.rec64, A.tri, A.n_tri, G, dxy, offx,
                                                           offy, offz, box_len, (int)ss, w,
                                                           4 * A.n_tri + 64, d_grid, m.stats);
   count_launch();

@@ -35,6 +35,7 @@
 // location it shares with the FP64 walk must round as the reference does;
 // the FP32 arithmetic asks for fused multiply-adds explicitly.
 #include <cfloat>
+#include <cstring>
 
 #include "mesh.h"
 
@@ -461,6 +462,14 @@ struct MapArgs32 {
   int* __restrict__ ray_status;
 };
 
+// One job of a batch launch: a range of one map's tiles.
+struct BatchJob32 {
+  MapArgs32 args;
+  long long first;  // first global tile of the job
+  int tile0;        // the job's first tile within its map
+  int count;        // tiles of this job
+};
+
 __device__ __forceinline__ void add_stats32(unsigned long long* stats, bool active, int crossed,
                                             int status, int fallbacks) {
   const unsigned mask = __activemask();
@@ -481,19 +490,14 @@ __device__ __forceinline__ void add_stats32(unsigned long long* stats, bool acti
   }
 }
 
-// Same tiling as k_map64: block = tile of pixels x samples, pixel means in
-// sample order from shared memory.  BLOCK threads per block and MINB blocks
-// per SM (the register budget) are compile-time; the autotuner picks among
-// the instantiations.
-template <int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_map32(const MapArgs32 a) {
-  extern __shared__ double s_val32[];  // P*S doubles, then P*S success bytes
-  __shared__ unsigned char s_lut[64];
-  fill_lut(s_lut);
-  __syncthreads();
+// One tile of one map: TW x TH pixels x S samples on BLOCK threads, one ray
+// per (pixel, sample), the S rays of a pixel in neighbouring lanes; the pixel
+// means are formed in sample order from shared memory (src/dtfe.c:615-645).
+template <int BLOCK>
+__device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
+                                           const unsigned char* __restrict__ lut, double* s_val,
+                                           unsigned char* s_ok) {
   const int P = a.TW * a.TH;
-  unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + P * a.S);
-  const int tile = blockIdx.x;
   const int tx0 = (tile % a.tiles_x) * a.TW, ty0 = (tile / a.tiles_x) * a.TH;
   for (int t = threadIdx.x; t < P * a.S; t += BLOCK) {
     const int lp = t / a.S, s = t % a.S;
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_map32(const MapArgs32 a) {
       int ft = -1;
       if (a.n_tri > 0) ft = locate64(a.tri, 0, xt, yt, a.loc_budget, &status);
       if (ft >= 0)
-        status = walk32(a.rec, a.C, ft, xt, yt, rid, s_lut, &v, &crossed, &fb, nullptr, 0);
+        status = walk32(a.rec, a.C, ft, xt, yt, rid, lut, &v, &crossed, &fb, nullptr, 0);
       if (status != kRayOk) v = 0.0;
       if (a.ray_rho) {
         a.ray_rho[rid] = v;
@@ -519,7 +523,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_map32(const MapArgs32 a) {
         a.ray_status[rid] = status;
       }
     }
-    s_val32[t] = v;
+    s_val[t] = v;
     s_ok[t] = crossed > 0;
     add_stats32(a.stats, active, crossed, status, fb);
   }
@@ -530,10 +534,68 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_map32(const MapArgs32 a) {
     double total = 0.0;
     int n_avg = 0;
     for (int s = 0; s < a.S; ++s) {
-      total += s_val32[lp * a.S + s];
+      total += s_val[lp * a.S + s];
       n_avg += s_ok[lp * a.S + s];
     }
     a.map[(size_t)row * a.G + col] += n_avg > 0 ? total / n_avg : 0.0;
+  }
+}
+
+// One block per tile.  BLOCK threads per block and MINB blocks per SM (the
+// register budget) are compile-time; the autotuner picks among the
+// instantiations.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_map32(const MapArgs32 a) {
+  extern __shared__ double s_val32[];  // P*S doubles, then P*S success bytes
+  __shared__ unsigned char s_lut[64];
+  fill_lut(s_lut);
+  __syncthreads();
+  unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + a.TW * a.TH * a.S);
+  map_tile32<BLOCK>(a, blockIdx.x, s_lut, s_val32, s_ok);
+}
+
+// Persistent batch: the blocks of one launch pull tiles from a device counter
+// across every job of the batch (maps of different meshes, sides and sample
+// counts), so uneven maps share the GPU without a tail per map.  Job j owns
+// global tiles [first[j], first[j+1]) and maps them to its own tiles
+// [tile0, tile0 + count).  The job's arguments are staged in shared memory.
+template <int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_batch32(const BatchJob32* __restrict__ jobs, int n_jobs, long long total_tiles,
+              unsigned long long* __restrict__ queue) {
+  extern __shared__ double s_val32[];
+  __shared__ unsigned char s_lut[64];
+  __shared__ MapArgs32 s_args;
+  __shared__ long long s_tile;
+  __shared__ int s_job;
+  fill_lut(s_lut);
+  int cur_job = -1;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_tile = (long long)atomicAdd(queue, 1ull);
+      int lo = 0, hi = n_jobs - 1;  // last job whose first tile <= s_tile
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (jobs[mid].first <= s_tile) lo = mid;
+        else hi = mid - 1;
+      }
+      s_job = lo;
+    }
+    __syncthreads();
+    const long long tile = s_tile;
+    const int j = s_job;
+    if (tile >= total_tiles) break;
+    if (j != cur_job) {  // stage the job's arguments
+      const int* src = reinterpret_cast<const int*>(&jobs[j].args);
+      int* dst = reinterpret_cast<int*>(&s_args);
+      for (int k = threadIdx.x; k < (int)(sizeof(MapArgs32) / sizeof(int)); k += BLOCK)
+        dst[k] = src[k];
+      cur_job = j;
+    }
+    __syncthreads();
+    unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + s_args.TW * s_args.TH * s_args.S);
+    map_tile32<BLOCK>(s_args, jobs[j].tile0 + (int)(tile - jobs[j].first), s_lut, s_val32, s_ok);
+    __syncthreads();  // s_val, s_args and s_tile are reused by the next tile
   }
 }
 
@@ -561,7 +623,7 @@ __global__ void __launch_bounds__(128) k_trace32(const TetRec32* __restrict__ re
   status[i] = st;
 }
 
-MixConf mix_conf(const Mesh& m, double z0, double lz, double dist, uint64_t seed,
+MixConf mix_conf(const Mesh& m, int axis, double z0, double lz, double dist, uint64_t seed,
                  int max_visits) {
   MixConf C;
   C.lz = lz;
@@ -575,7 +637,7 @@ MixConf mix_conf(const Mesh& m, double z0, double lz, double dist, uint64_t seed
   C.dist = dist;
   C.seed = seed;
   C.max_visits = max_visits;
-  C.rec64 = m.rec64;
+  C.rec64 = m.ax[axis].rec64;
   C.exact32 = m.fp32_exact ? 1 : 0;
   return C;
 }
@@ -612,18 +674,32 @@ const Variant32 kVariants32[] = {
 constexpr int kNumVariants32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
 constexpr int kDefaultVariant32 = 1;  // (256, 3): the usual winner on B200
 
-}  // namespace
+typedef void (*BatchKernel32)(const BatchJob32*, int, long long, unsigned long long*);
+const BatchKernel32 kBatch32[] = {k_batch32<256, 2>, k_batch32<256, 3>, k_batch32<256, 4>,
+                                  k_batch32<128, 4>, k_batch32<128, 6>, k_batch32<256, 2>,
+                                  k_batch32<256, 3>};
+static_assert(sizeof(kBatch32) / sizeof(kBatch32[0]) == kNumVariants32, "one batch kernel per variant");
 
-dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
-                           double* ray_rho, int* ray_crossed, int* ray_status) {
-  if (!m.rec32) return set_error(DTFE_ERR_INVALID, "mixed map without FP32 records");
-  if (!m.fp32_exact && !m.rec64)
+// Checks that an axis has what the mixed walk reads.
+dtfe_status_t check_mixed(const Mesh& m, int axis) {
+  const AxisData& A = m.ax[axis];
+  if (!A.rec32 || !A.hull_built) return set_error(DTFE_ERR_INVALID, "mixed walk without FP32 records");
+  if (!m.fp32_exact && !A.rec64)
     return set_error(DTFE_ERR_INVALID, "coordinates are not floats and no FP64 records are kept");
-  const AxisData& A = m.ax[m.rec_axis];
-  const int vi = (m.tune32 >= 0 && m.tune32 < kNumVariants32) ? m.tune32 : kDefaultVariant32;
+  return DTFE_OK;
+}
+
+int pick_variant32(int v) { return (v >= 0 && v < kNumVariants32) ? v : kDefaultVariant32; }
+
+// The kernel arguments of one mixed map; *tiles_y receives its rows of tiles.
+dtfe_status_t map_args32(Mesh& m, const MapGeom& g, int vi, double* d_map,
+                         unsigned long long* stats, double* ray_rho, int* ray_crossed,
+                         int* ray_status, MapArgs32* out, int* tiles_y) {
+  SDTFE_TRY(check_mixed(m, g.axis));
+  const AxisData& A = m.ax[g.axis];
   const Variant32& V = kVariants32[vi];
-  MapArgs32 a;
-  a.rec = m.rec32;
+  MapArgs32& a = *out;
+  a.rec = A.rec32;
   a.tri = A.tri;
   a.n_tri = A.n_tri;
   a.map = d_map;
@@ -631,18 +707,30 @@ dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   a.S = g.S;
   tile_shape32(V.block, g.S, V.wide, &a.TW, &a.TH);
   a.tiles_x = (g.G + a.TW - 1) / a.TW;
-  const int tiles_y = (g.G + a.TH - 1) / a.TH;
+  *tiles_y = (g.G + a.TH - 1) / a.TH;
   a.dxy = g.dxy;
   a.offx = g.offx;
   a.offy = g.offy;
   a.scale = g.scale;
   a.soff = g.soff;
-  a.C = mix_conf(m, g.offz, g.lz, g.dist, g.seed, g.max_visits);
+  a.C = mix_conf(m, g.axis, g.offz, g.lz, g.dist, g.seed, g.max_visits);
   a.loc_budget = 4 * A.n_tri + 64;
-  a.stats = m.stats;
+  a.stats = stats;
   a.ray_rho = ray_rho;
   a.ray_crossed = ray_crossed;
   a.ray_status = ray_status;
+  return DTFE_OK;
+}
+
+}  // namespace
+
+dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_t s,
+                           double* ray_rho, int* ray_crossed, int* ray_status) {
+  const int vi = pick_variant32(m.tune32);
+  const Variant32& V = kVariants32[vi];
+  MapArgs32 a;
+  int tiles_y = 0;
+  SDTFE_TRY(map_args32(m, g, vi, d_map, m.stats, ray_rho, ray_crossed, ray_status, &a, &tiles_y));
   const size_t smem = (size_t)a.TW * a.TH * g.S * (sizeof(double) + 1);
   if (smem > 40 * 1024)
     SDTFE_CUDA(cudaFuncSetAttribute(V.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -657,17 +745,15 @@ dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   return DTFE_OK;
 }
 
-dtfe_status_t launch_trace32(Mesh& m, int n_rays, const double* d_x, const double* d_y, double z0,
-                             double lz, double dxy, uint64_t seed, int max_visits, double* d_rho,
-                             int* d_crossed, int* d_status, int* d_visits, int max_record,
-                             cudaStream_t s) {
-  if (!m.rec32) return set_error(DTFE_ERR_INVALID, "mixed trace without FP32 records");
-  if (!m.fp32_exact && !m.rec64)
-    return set_error(DTFE_ERR_INVALID, "coordinates are not floats and no FP64 records are kept");
-  const AxisData& A = m.ax[m.rec_axis];
-  MixConf C = mix_conf(m, z0, lz, (dxy / 2.0) / kPerturbMax, seed, max_visits);
+dtfe_status_t launch_trace32(Mesh& m, int axis, int n_rays, const double* d_x, const double* d_y,
+                             double z0, double lz, double dxy, uint64_t seed, int max_visits,
+                             double* d_rho, int* d_crossed, int* d_status, int* d_visits,
+                             int max_record, cudaStream_t s) {
+  SDTFE_TRY(check_mixed(m, axis));
+  const AxisData& A = m.ax[axis];
+  MixConf C = mix_conf(m, axis, z0, lz, (dxy / 2.0) / kPerturbMax, seed, max_visits);
   if (n_rays > 0) {
-    k_trace32<<<(n_rays + 127) / 128, 128, 0, s>>>(m.rec32, A.tri, A.n_tri, n_rays, d_x, d_y, C,
+    k_trace32<<<(n_rays + 127) / 128, 128, 0, s>>>(A.rec32, A.tri, A.n_tri, n_rays, d_x, d_y, C,
                                                    4 * A.n_tri + 64, d_rho, d_crossed, d_status,
                                                    d_visits, max_record);
     count_launch();
@@ -679,6 +765,78 @@ dtfe_status_t launch_trace32(Mesh& m, int n_rays, const double* d_x, const doubl
 }  // namespace sdtfe
 
 namespace sdtfe {
+int default_variant32() { return kDefaultVariant32; }
+
+int map_tiles32(const MapGeom& g, int variant) {
+  const Variant32& V = kVariants32[pick_variant32(variant)];
+  int TW, TH;
+  tile_shape32(V.block, g.S, V.wide, &TW, &TH);
+  return ((g.G + TW - 1) / TW) * ((g.G + TH - 1) / TH);
+}
+
+dtfe_status_t plan_batch32(const BatchMap* maps, int n, int variant, BatchPlan* plan) {
+  const int vi = pick_variant32(variant);
+  plan->precision = DTFE_MIXED;
+  plan->variant = vi;
+  plan->n_jobs = 0;
+  plan->total_tiles = 0;
+  plan->smem = 0;
+  plan->jobs.assign(sizeof(BatchJob32) * (size_t)(n > 0 ? n : 0), 0);
+  for (int i = 0; i < n; ++i) {
+    const BatchMap& b = maps[i];
+    BatchJob32 j;
+    int tiles_y = 0;
+    SDTFE_TRY(map_args32(*b.mesh, b.g, vi, b.d_map, b.stats, nullptr, nullptr, nullptr, &j.args,
+                         &tiles_y));
+    const long long tiles = (long long)j.args.tiles_x * tiles_y;
+    const long long cnt = b.count < 0 ? tiles - b.tile0 : b.count;
+    if (b.tile0 < 0 || cnt < 0 || b.tile0 + cnt > tiles)
+      return set_error(DTFE_ERR_INVALID, "batch map %d: tiles [%d, %lld) outside the map's %lld", i,
+                       b.tile0, b.tile0 + cnt, tiles);
+    if (cnt == 0) continue;
+    j.first = plan->total_tiles;
+    j.tile0 = b.tile0;
+    j.count = (int)cnt;
+    memcpy(plan->jobs.data() + sizeof(BatchJob32) * plan->n_jobs, &j, sizeof(j));
+    ++plan->n_jobs;
+    plan->total_tiles += cnt;
+    const size_t smem = (size_t)j.args.TW * j.args.TH * j.args.S * (sizeof(double) + 1);
+    if (smem > plan->smem) plan->smem = smem;
+  }
+  plan->jobs.resize(sizeof(BatchJob32) * plan->n_jobs);
+  return DTFE_OK;
+}
+
+dtfe_status_t batch_grid32(int variant, size_t smem, int* grid, int* block) {
+  const int vi = pick_variant32(variant);
+  int dev = 0, sms = 0, per_sm = 0;
+  SDTFE_CUDA(cudaGetDevice(&dev));
+  SDTFE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (smem > 40 * 1024)
+    SDTFE_CUDA(cudaFuncSetAttribute(kBatch32[vi], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  SDTFE_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kBatch32[vi], kVariants32[vi].block,
+                                                           smem));
+  if (per_sm < 1)
+    return set_error(DTFE_ERR_UNSUPPORTED, "mixed batch: %zu B of shared memory per block", smem);
+  *grid = per_sm * sms;
+  *block = kVariants32[vi].block;
+  return DTFE_OK;
+}
+
+dtfe_status_t launch_batch32(const BatchPlan& plan, const void* d_jobs, unsigned long long* d_queue,
+                             int grid, cudaStream_t s) {
+  if (plan.n_jobs == 0) return DTFE_OK;
+  const int vi = pick_variant32(plan.variant);
+  if (plan.smem > 40 * 1024)
+    SDTFE_CUDA(cudaFuncSetAttribute(kBatch32[vi], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)plan.smem));
+  kBatch32[vi]<<<grid, kVariants32[vi].block, plan.smem, s>>>(
+      static_cast<const BatchJob32*>(d_jobs), plan.n_jobs, plan.total_tiles, d_queue);
+  count_launch();
+  SDTFE_CUDA(cudaGetLastError());
+  return DTFE_OK;
+}
+
 int num_map32_variants() { return kNumVariants32; }
 void map32_variant_info(int i, int* block, int* minb, int* wide) {
   *block = kVariants32[i].block;

@@ -105,3 +105,29 @@ def perturbed_lattice(n_side=192, sigma_frac=0.3, extra_frac=0.3, n_clusters=200
     n_extra = int(round(extra_frac * len(lat)))
     c = clusters_r2(rng, n_extra, n_clusters, r_max, rng.random((n_clusters, 3)))
     return _rows(np.concatenate([lat, c]) % 1.0, f32=True)
+
+
+@dataclass
+class Request:
+    t: float          # arrival time, seconds from the start of the stream
+    cutout: int
+    axis: int
+    spec: MapSpec
+
+
+def serving_stream(n_cutouts=256, n_min=10_000, n_max=2_000_000, n_requests=512, rate=100.0,
+                   seed=4, sides=(128, 256, 512, 1024, 2048), s_min=4, s_max=16):
+    """Serving stream: particle counts of the resident cutouts (log-uniform in
+    [n_min, n_max]) and a Poisson arrival trace at `rate` requests/s; each
+    request draws a cutout, a projection axis (z, x, y), a map side from
+    `sides` and s_min..s_max samples per pixel.  Cutouts are built with
+    halo_cutout(n, seed * 1000 + i); maps cover the 2 x 2 x 2 cube."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_cutouts)).astype(int)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    reqs = []
+    for k in range(n_requests):
+        spec = MapSpec(int(rng.choice(sides)), int(rng.integers(s_min, s_max + 1)), 2.0, 2.0,
+                       (0.0, 0.0, 0.0))
+        reqs.append(Request(float(t[k]), int(rng.integers(n_cutouts)), int(rng.integers(3)), spec))
+    return ns, reqs
