@@ -27,6 +27,19 @@ start of the step, as callers of compute_density do).  Reported:
                 sources into oracle/_ref, OpenMP on all host cores) on a
                 sub-window of the same map with the same pixel size
 
+Sections (N=1; --sections none skips them), host Qhull for all of them in a
+spawn process pool before CUDA starts:
+
+  batch         64 halo cutouts (N log-uniform in [1e4, 5e5]), one map each
+                (sides 256/512/1024, 8 samples/pixel) in one persistent launch
+                captured in a CUDA graph, autotuned; against one launch per
+                map and against the FP64 batch (speed-up, max/RMS error)
+  serving       map requests (random cutout, axis, side 128..2048, 4-16
+                samples/pixel) through the serving loop over --serve-handles
+                resident cutouts: closed-loop capacity in rays/s, then Poisson
+                arrivals at --serve-load of that capacity, p50/p99 latency,
+                mixed vs FP64 and the mixed maps' error
+
 --impl reference runs only the reference's CPU implementation (same metric).
 Multi-GPU (torchrun, --gpus N): replicas; each rank maps its own copy of the
 workload, value = all ranks' rays / the slowest rank's time.
@@ -62,6 +75,14 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--sections", default="batch,serving",
+                    help="extra sections on one GPU: batch (64 cutouts in one persistent launch), "
+                         "serving (request stream with continuous batching); 'none' to skip")
+    ap.add_argument("--serve-handles", type=int, default=256)
+    ap.add_argument("--serve-distinct", type=int, default=32)
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--serve-load", type=float, default=0.7,
+                    help="Poisson arrival rate as a fraction of the measured mixed capacity")
     return ap.parse_args()
 
 
@@ -78,6 +99,41 @@ def workload(name):
         pos4, spec = W.clustered_box()
         desc = "clustered_1M_2048x16"
     return desc, pos4, spec
+
+
+def _qhull_task(task):
+    """One host triangulation (spawned worker): builds the particle set from
+    its generator and seed, then Qhull + the library's layout step."""
+    kind, key, n, seed = task
+    import sdtfe_b200 as sd
+    from sdtfe_b200 import workloads as W
+
+    if kind == "main":
+        pos4 = workload(key)[1]
+    elif kind == "cutout":
+        pos4 = W.halo_cutout(n, seed)
+    else:  # "clustered": the clustered-box recipe at n particles
+        pos4 = W.clustered_box(n=n, seed=seed)[0]
+    t = time.perf_counter()
+    tetra = sd.triangulate(pos4)
+    return kind, key, pos4, tetra, time.perf_counter() - t
+
+
+def triangulate_all(tasks):
+    """Runs the Qhull tasks in a spawn process pool, largest first.  Called
+    before the first CUDA call of the process."""
+    import multiprocessing as mp
+
+    procs = max(1, min(len(tasks), len(os.sched_getaffinity(0)), 32))
+    order = sorted(tasks, key=lambda t: -t[2])
+    out, cpu_s = {}, 0.0
+    t = time.perf_counter()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        for kind, key, pos4, tetra, dt in pool.imap_unordered(_qhull_task, order, chunksize=1):
+            out[(kind, key)] = (pos4, tetra, dt)
+            cpu_s += dt
+    return out, {"procs": procs, "wall_s": round(time.perf_counter() - t, 1),
+                 "cpu_s": round(cpu_s, 1)}
 
 
 # ---------------------------------------------------------------------------
@@ -248,7 +304,225 @@ def read_ncu_traffic(kernel, n_tets):
         return None
 
 
-def run_ours(args):
+def plan_sections(args):
+    """Qhull for the main workload and the sections, in a process pool, before
+    any CUDA call (sections run at N=1 only)."""
+    from sdtfe_b200 import workloads as W
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    sections = [] if args.sections == "none" or world > 1 else args.sections.split(",")
+    if not sections:
+        return None
+    n_main = {"uniform": 32768, "clustered_262k": 1 << 18}.get(args.workload, 1 << 20)
+    tasks = [("main", args.workload, n_main, 0)]
+    if "batch" in sections:
+        tasks += [("cutout", i, n, seed) for i, (n, seed, _) in enumerate(W.cutout_specs())]
+    if "serving" in sections:
+        tasks += [("clustered", i, n, seed)
+                  for i, (n, seed) in enumerate(W.serving_cutouts(args.serve_distinct))]
+    tri, qinfo = triangulate_all(tasks)
+    return tri, qinfo, sections
+
+
+def timed_launches(torch, stream, flush, fn, steps):
+    """CUDA-event time (ms) of each of `steps` calls of fn on `stream`, the L2
+    flushed before each."""
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    for a, b in ev:
+        flush.zero_()
+        a.record(stream)
+        fn()
+        b.record(stream)
+    torch.cuda.synchronize()
+    return np.array([a.elapsed_time(b) for a, b in ev])
+
+
+def max_rel(got, want):
+    ok = np.abs(want) > 0
+    r = np.abs(got - want)[ok] / np.abs(want[ok])
+    return float(r.max()) if r.size else 0.0, float(np.sqrt(np.mean(r ** 2))) if r.size else 0.0
+
+
+def section_batch(args, sd, torch, dev, stream, flush, tri):
+    """64 halo cutouts, one map each, in one persistent launch captured in a
+    CUDA graph; against the same maps launched one by one, and the FP64
+    batch.  Inputs resident; each step zeroes the maps (inside the graph)."""
+    from sdtfe_b200 import workloads as W
+
+    specs = W.cutout_specs()
+    meshes, p32, p64, d32, d64 = [], [], [], [], []
+    for i, (n, seed, sp) in enumerate(specs):
+        pos4, tetra, _ = tri[("cutout", i)]
+        meshes.append(sd.Mesh(pos4, tetra, 1.0))
+        kw = dict(seed=5000 + i)
+        p32.append(sd.map_params(sp.grid_dim, sp.box_len, sp.box_len_z, sp.center, sp.n_samples,
+                                 precision=sd.DTFE_MIXED, **kw))
+        p64.append(sd.map_params(sp.grid_dim, sp.box_len, sp.box_len_z, sp.center, sp.n_samples,
+                                 precision=sd.DTFE_FP64, **kw))
+        d32.append(torch.zeros(sp.grid_dim ** 2, dtype=torch.float64, device=dev))
+        d64.append(torch.zeros(sp.grid_dim ** 2, dtype=torch.float64, device=dev))
+    rays = sum(sp.rays for _, _, sp in specs)
+    sptr = stream.cuda_stream
+    flags = sd.BATCH_GRAPH | sd.BATCH_ZERO_MAPS
+    b32 = sd.Batch(list(zip(meshes, p32, [d.data_ptr() for d in d32])), flags)
+    best, table = b32.autotune()
+    for _ in range(args.warmup):
+        b32.launch(sptr)
+    torch.cuda.synchronize()
+    launches0 = sd.lib().dtfe_kernel_launches()
+    ms = timed_launches(torch, stream, flush, lambda: b32.launch(sptr), args.steps)
+    launches = sd.lib().dtfe_kernel_launches() - launches0
+    st32 = b32.stats()
+    info = b32.info()
+
+    def one_by_one():  # the same 64 maps, one launch per map, default kernel variant
+        for m, p, d in zip(meshes, p32, d32):
+            d.zero_()
+            m.map_device(p, d.data_ptr(), sptr)
+    one_by_one()
+    ms_seq = timed_launches(torch, stream, flush, one_by_one, 2)
+    # FP64 batch and the mixed maps' error against it
+    b64 = sd.Batch(list(zip(meshes, p64, [d.data_ptr() for d in d64])), flags)
+    b64.launch(sptr)
+    ms64 = timed_launches(torch, stream, flush, lambda: b64.launch(sptr), 2)
+    st64 = b64.stats()
+    b32.launch(sptr)
+    torch.cuda.synchronize()
+    errs = [max_rel(a.cpu().numpy(), b.cpu().numpy()) for a, b in zip(d32, d64)]
+    # end to end: the graph launch plus every map to pinned host memory
+    host = [torch.empty(d.numel(), dtype=torch.float64).pin_memory() for d in d32]
+
+    def e2e():
+        b32.launch(sptr)
+        for h, d in zip(host, d32):
+            h.copy_(d, non_blocking=True)
+    e2e()
+    ms_e2e = timed_launches(torch, stream, flush, e2e, 2)
+    visits = sum(x.visits for x in st32)
+    out = {
+        "workload": "64 halo cutouts, N log-uniform [1e4, 5e5] (r^-2 cluster + 20% background), "
+                    "sides {256,512,1024}, 8 samples/pixel, one persistent launch in a CUDA graph",
+        "particles": int(sum(n for n, _, _ in specs)),
+        "tets": int(sum(m.info().n_tetra for m in meshes)),
+        "rays_per_step": int(rays),
+        "rays_per_s": rays / (np.median(ms) / 1e3),
+        "ms_per_step": float(np.median(ms)),
+        "maps_per_s": len(specs) / (np.median(ms) / 1e3),
+        "one_launch_per_map_rays_per_s": rays / (np.median(ms_seq) / 1e3),
+        "fp64_batch_rays_per_s": rays / (np.median(ms64) / 1e3),
+        "speedup_mixed_over_fp64": float(np.median(ms64) / np.median(ms)),
+        "max_rel_err": max(e[0] for e in errs),
+        "rms_rel_err": float(np.sqrt(np.mean([e[1] ** 2 for e in errs]))),
+        "visits_equal_fp64": bool(visits == sum(x.visits for x in st64)),
+        "visits_per_ray": visits / rays,
+        "e2e_rays_per_s": rays / (np.median(ms_e2e) / 1e3),
+        "e2e_d2h_bytes_per_step": int(sum(d.numel() * 8 for d in d32)),
+        "grid": info["grid"], "block": info["block"], "tiles": info["tiles"],
+        "autotune": {"chosen": best, "ms": [round(t["ms"], 3) for t in table]},
+        "gpu_launches": int(launches),
+    }
+    b32.close()
+    b64.close()
+    for m in meshes:
+        m.close()
+    return out
+
+
+def _run_stream(sd, srv, ids, reqs, precision, rate, keep=None, compare=None):
+    """Replays `reqs` against the server: open loop at `rate` requests/s
+    (inter-arrival times of the trace rescaled), or all at t=0 when rate is
+    None.  Returns latency percentiles and the achieved rays/s."""
+    t0 = time.perf_counter()
+    scale = (len(reqs) / rate) / reqs[-1].t if rate is not None else None
+    rids = []
+    for k, r in enumerate(reqs):
+        if scale is not None:
+            due = t0 + r.t * scale
+            while True:
+                now = time.perf_counter()
+                if now >= due:
+                    break
+                time.sleep(min(due - now, 0.002))
+        sp = r.spec
+        p = sd.map_params(sp.grid_dim, sp.box_len, sp.box_len_z, sp.center, sp.n_samples,
+                          seed=7000 + k, axis=r.axis, precision=precision)
+        rids.append(srv.submit(ids[r.cutout], p))
+    lat, rays, errs, vis_eq, worst = [], 0, [], True, None
+    for k, rid in enumerate(rids):
+        m, info = srv.wait(rid)
+        lat.append(info.latency_ms)
+        rays += info.stats.rays
+        if keep is not None:
+            keep[k] = (m, info.stats.visits)
+        if compare is not None:
+            w, wv = compare[k]
+            e = max_rel(w, m)  # the mixed map against this FP64 one
+            errs.append(e)
+            if worst is None or e[0] > worst[0]:
+                r = reqs[k]
+                worst = (e[0], {"request": k, "cutout": r.cutout, "axis": r.axis,
+                                "side": r.spec.grid_dim, "samples": r.spec.n_samples})
+            vis_eq = vis_eq and wv == info.stats.visits
+    wall = time.perf_counter() - t0
+    lat = np.array(lat)
+    out = {"requests": len(reqs), "rays": int(rays), "wall_s": round(wall, 3),
+           "rays_per_s": rays / wall,
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "max_ms": float(lat.max())}
+    if rate is not None:
+        out["rate_per_s"] = rate
+    if errs:
+        out["max_rel_err_mixed_vs_fp64"] = max(e[0] for e in errs)
+        out["rms_rel_err_mixed_vs_fp64"] = float(np.sqrt(np.mean([e[1] ** 2 for e in errs])))
+        out["worst_request"] = worst[1]
+        out["visits_equal_fp64"] = bool(vis_eq)
+    return out
+
+
+def section_serving(args, sd, torch, tri):
+    """Map requests over many resident cutouts through the serving loop:
+    closed-loop capacity (all requests at once) and open-loop Poisson arrivals
+    at a fraction of the mixed capacity, mixed vs FP64."""
+    from sdtfe_b200 import workloads as W
+
+    cut = W.serving_cutouts(args.serve_distinct)
+    meshes = []
+    for h in range(args.serve_handles):
+        pos4, tetra, _ = tri[("clustered", h % len(cut))]
+        meshes.append(sd.Mesh(pos4, tetra, 1.0))
+    _, reqs = W.serving_stream(n_cutouts=args.serve_handles, n_requests=args.serve_requests)
+    out = {"workload": f"{args.serve_handles} resident cutouts ({len(cut)} distinct "
+                       "clustered-box triangulations, N log-uniform [1e4, 5e5]); "
+                       f"{len(reqs)} requests: random cutout, axis, side in "
+                       "{128..2048}, 4-16 samples/pixel",
+           "particles_resident": int(sum(cut[h % len(cut)][0] for h in range(args.serve_handles)))}
+    with sd.Server() as srv:
+        ids = [srv.add_mesh(m) for m in meshes]
+        # warm-up: one small request per cutout touches every handle once
+        warm = [srv.submit(i, sd.map_params(32, 1.0, 1.0, (0.5, 0.5, 0.5), 1, seed=1,
+                                            precision=sd.DTFE_MIXED)) for i in ids]
+        for w in warm:
+            srv.wait(w)
+        keep = {}
+        out["capacity_mixed"] = _run_stream(sd, srv, ids, reqs, sd.DTFE_MIXED, None, keep=keep)
+        out["capacity_fp64"] = _run_stream(sd, srv, ids, reqs, sd.DTFE_FP64, None, compare=keep)
+        keep.clear()
+        rate = args.serve_load * len(reqs) / out["capacity_mixed"]["wall_s"]
+        out["poisson_mixed"] = _run_stream(sd, srv, ids, reqs, sd.DTFE_MIXED, rate)
+        out["poisson_fp64"] = _run_stream(sd, srv, ids, reqs, sd.DTFE_FP64, rate)
+        st = srv.stats()
+        out["server"] = {"iterations": st.iterations, "evictions": st.evictions,
+                         "budget_gb": st.budget / 1e9, "peak_gb": st.peak / 1e9,
+                         "completed": st.completed, "failed": st.failed}
+    out["speedup_mixed_over_fp64"] = (out["capacity_mixed"]["rays_per_s"] /
+                                      out["capacity_fp64"]["rays_per_s"])
+    for m in meshes:
+        m.close()
+    return out
+
+
+def run_ours(args, pre=None):
     import torch
 
     import sdtfe_b200 as sd
@@ -268,9 +542,15 @@ def run_ours(args):
     dev = torch.device("cuda", local)
 
     desc, pos4, spec = workload(args.workload)
-    t = time.perf_counter()
-    tetra = sd.triangulate(pos4)
-    t_qhull = time.perf_counter() - t
+    tri = sections = None
+    if pre is not None:  # host Qhull ran in the process pool before CUDA started
+        tri, qinfo, sections = pre
+        _, tetra, t_qhull = tri[("main", args.workload)]
+    else:
+        t = time.perf_counter()
+        tetra = sd.triangulate(pos4)
+        t_qhull = time.perf_counter() - t
+        qinfo, sections = None, []
     prec = sd.DTFE_MIXED if args.precision == "mixed" else sd.DTFE_FP64
     mesh = sd.Mesh(pos4, tetra, 1.0)
     G, S = spec.grid_dim, spec.n_samples
@@ -414,6 +694,14 @@ def run_ours(args):
             cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
 
+    extra = {}
+    if sections and "batch" in sections:
+        extra["batch"] = section_batch(args, sd, torch, dev, stream, flush, tri)
+    if sections and "serving" in sections:
+        extra["serving"] = section_serving(args, sd, torch, tri)
+    if qinfo:
+        extra["qhull_pool"] = qinfo
+
     if rank == 0:
         line = {
             "metric": "los_rays_per_s", "value": value, "unit": "rays/s", "n_gpus": world,
@@ -451,6 +739,7 @@ def run_ours(args):
             "clocks": clk,
             "gpu_launches": int(launches),
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     mesh.close()
     if dist:
@@ -463,7 +752,7 @@ def main():
     if args.impl == "reference":
         run_reference(args)
     else:
-        run_ours(args)
+        run_ours(args, plan_sections(args))
 
 
 if __name__ == "__main__":

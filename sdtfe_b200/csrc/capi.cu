@@ -54,7 +54,9 @@ dtfe_status_t check_params(const Mesh& m, const dtfe_map_params_t* p) {
 // records + hull for the map's axis and precision, on the mesh stream
 dtfe_status_t prepare_axis(Mesh& m, int axis, int precision) {
   if (!m.grad) SDTFE_TRY(mesh_gradients(&m));
-  const bool want64 = precision == DTFE_FP64 || !(m.flags & DTFE_MESH_NO_FP64_REC);
+  // the mixed walk reads FP64 records only when the coordinates are not floats
+  const bool want64 = precision == DTFE_FP64 ||
+                      (!m.fp32_exact && !(m.flags & DTFE_MESH_NO_FP64_REC));
   const bool want32 = precision == DTFE_MIXED;
   SDTFE_TRY(mesh_records(&m, axis, want64, want32));
   SDTFE_TRY(mesh_hull(&m, axis, nullptr, nullptr));

@@ -121,7 +121,8 @@ size_t missing_record_bytes(const Mesh& m, int axis, int precision) {
   const AxisData& A = m.ax[axis];
   size_t b = 0;
   if (precision == DTFE_MIXED && !A.rec32) b += kRec32Bytes * (size_t)m.nt;
-  const bool want64 = precision == DTFE_FP64 || !(m.flags & DTFE_MESH_NO_FP64_REC);
+  const bool want64 = precision == DTFE_FP64 ||
+                      (!m.fp32_exact && !(m.flags & DTFE_MESH_NO_FP64_REC));
   if (want64 && !A.rec64) b += kRec64Bytes * (size_t)m.nt;
   return b;
 }

@@ -78,18 +78,23 @@ def halo_cutout(n, seed, bg_frac=0.2, r_max=1.0):
     return _rows(np.concatenate([cl, bg]), f32=True)
 
 
-def cutout_batch(n_cutouts=64, n_min=10_000, n_max=500_000, seed=3, sides=(256, 512, 1024),
+def cutout_specs(n_cutouts=64, n_min=10_000, n_max=500_000, seed=3, sides=(256, 512, 1024),
                  n_samples=8):
-    """Batched cutouts: counts log-uniform in [n_min, n_max], map side drawn
-    uniformly from `sides`, box 2 x 2 x 2 about the origin."""
+    """Batched cutouts: (particle count, cutout seed, map) per cutout; counts
+    log-uniform in [n_min, n_max], map side drawn uniformly from `sides`, box
+    2 x 2 x 2 about the origin.  The particles are halo_cutout(n, seed)."""
     rng = np.random.default_rng(seed)
     ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_cutouts)).astype(int)
     out = []
     for i, n in enumerate(ns):
         side = int(rng.choice(sides))
-        out.append((halo_cutout(int(n), seed * 1000 + i),
-                    MapSpec(side, n_samples, 2.0, 2.0, (0.0, 0.0, 0.0))))
+        out.append((int(n), seed * 1000 + i, MapSpec(side, n_samples, 2.0, 2.0, (0.0, 0.0, 0.0))))
     return out
+
+
+def cutout_batch(**kw):
+    """cutout_specs with the particles generated: [(pos4, MapSpec)]."""
+    return [(halo_cutout(n, s), spec) for n, s, spec in cutout_specs(**kw)]
 
 
 def perturbed_lattice(n_side=192, sigma_frac=0.3, extra_frac=0.3, n_clusters=2000, r_max=0.01,
@@ -120,14 +125,24 @@ def serving_stream(n_cutouts=256, n_min=10_000, n_max=2_000_000, n_requests=512,
     """Serving stream: particle counts of the resident cutouts (log-uniform in
     [n_min, n_max]) and a Poisson arrival trace at `rate` requests/s; each
     request draws a cutout, a projection axis (z, x, y), a map side from
-    `sides` and s_min..s_max samples per pixel.  Cutouts are built with
-    halo_cutout(n, seed * 1000 + i); maps cover the 2 x 2 x 2 cube."""
+    `sides` and s_min..s_max samples per pixel.  Cutouts are built like the
+    clustered single map, clustered_box(n, seed * 1000 + i); maps cover the
+    unit box."""
     rng = np.random.default_rng(seed)
     ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_cutouts)).astype(int)
     t = np.cumsum(rng.exponential(1.0 / rate, n_requests))
     reqs = []
     for k in range(n_requests):
-        spec = MapSpec(int(rng.choice(sides)), int(rng.integers(s_min, s_max + 1)), 2.0, 2.0,
-                       (0.0, 0.0, 0.0))
+        spec = MapSpec(int(rng.choice(sides)), int(rng.integers(s_min, s_max + 1)), 1.0, 1.0,
+                       (0.5, 0.5, 0.5))
         reqs.append(Request(float(t[k]), int(rng.integers(n_cutouts)), int(rng.integers(3)), spec))
     return ns, reqs
+
+
+def serving_cutouts(n_distinct=32, n_min=10_000, n_max=500_000, seed=4):
+    """Particle counts (log-uniform in [n_min, n_max]) and seeds of the
+    distinct cutout triangulations behind the serving stream's handles;
+    handle i holds its own device copy of cutout i % n_distinct."""
+    rng = np.random.default_rng(seed + 17)
+    ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_distinct)).astype(int)
+    return [(int(n), seed * 1000 + i) for i, n in enumerate(ns)]
