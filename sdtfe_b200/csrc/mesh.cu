@@ -7,6 +7,7 @@
 // and must not be contracted into fused multiply-adds.
 #include <cub/device/device_scan.cuh>
 
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -151,7 +152,8 @@ __global__ void k_gradients(const double4* __restrict__ pos, const int4* __restr
 // vertex densities (the mixed walk's barycentric form of the same field).
 __global__ void k_records(const double4* __restrict__ pos, const int4* __restrict__ rows,
                           const double* __restrict__ grad, int nt, int axis,
-                          TetRec64* __restrict__ r64, TetRec32* __restrict__ r32) {
+                          TetRec64* __restrict__ r64, TetRec32* __restrict__ r32,
+                          TetRot32* __restrict__ rot, int* __restrict__ hz_bits) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   const int4 v = rows[2 * (size_t)t];
@@ -184,6 +186,37 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
     r.nb = nb;
     r.aux = v;
     r32[t] = r;
+  }
+  if (rot) {
+    // the record of each neighbour as entered from this tet
+    const int nbo[4] = {nb.x, nb.y, nb.z, nb.w};
+    int nxt[4];
+    float zmin = (float)q[0][2], zmax = zmin;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      zmin = fminf(zmin, (float)q[s][2]);
+      zmax = fmaxf(zmax, (float)q[s][2]);
+      const int n = nbo[s];
+      if (n < 0) {
+        nxt[s] = -1;
+        continue;
+      }
+      const int4 m = rows[2 * (size_t)n + 1];
+      const int f = m.x == t ? 0 : (m.y == t ? 1 : (m.z == t ? 2 : (m.w == t ? 3 : -1)));
+      nxt[s] = f >= 0 ? 4 * n + f : INT_MIN;
+    }
+    atomicMax(hz_bits, __float_as_int(zmax - zmin));  // non-negative: int order = float order
+#pragma unroll
+    for (int F = 0; F < 4; ++F) {
+      const int s0 = rot_slot(F, 0), s1 = rot_slot(F, 1), s2 = rot_slot(F, 2), s3 = rot_slot(F, 3);
+      TetRot32 r;
+      r.xy01 = make_float4((float)q[s0][0], (float)q[s0][1], (float)q[s1][0], (float)q[s1][1]);
+      r.xy23 = make_float4((float)q[s2][0], (float)q[s2][1], (float)q[s3][0], (float)q[s3][1]);
+      r.z = make_float4((float)q[s0][2], (float)q[s1][2], (float)q[s2][2], (float)q[s3][2]);
+      r.fld = make_float4((float)p[s0].w, (float)p[s1].w, (float)p[s2].w, (float)p[s3].w);
+      r.nb = make_int4(nxt[s0], nxt[s1], nxt[s2], t);
+      rot[4 * (size_t)t + F] = r;
+    }
   }
 }
 
@@ -439,12 +472,28 @@ dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32) {
   const bool need64 = want64 && !A.rec64, need32 = want32 && !A.rec32;
   if (!need64 && !need32) return DTFE_OK;
   if (need64) SDTFE_TRY(dmalloc(&A.rec64, m->nt, m));
+  // rotated records address 4*t + F in an int: up to 2^29 - 1 tets
+  const bool need_rot = need32 && m->nt < (1 << 29);
   if (need32) SDTFE_TRY(dmalloc(&A.rec32, m->nt, m));
+  if (need_rot) SDTFE_TRY(dmalloc(&A.rot32, 4 * (size_t)m->nt, m));
   if (m->nt) {
+    int* hz = nullptr;
+    if (need_rot) {
+      SDTFE_CUDA(cudaMallocAsync(&hz, sizeof(int), m->stream));
+      SDTFE_CUDA(cudaMemsetAsync(hz, 0, sizeof(int), m->stream));
+    }
     k_records<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, axis,
                                                          need64 ? A.rec64 : nullptr,
-                                                         need32 ? A.rec32 : nullptr);
+                                                         need32 ? A.rec32 : nullptr,
+                                                         need_rot ? A.rot32 : nullptr, hz);
     count_launch();
+    if (need_rot) {
+      int bits = 0;
+      SDTFE_CUDA(cudaMemcpyAsync(&bits, hz, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+      cudaFreeAsync(hz, m->stream);
+      SDTFE_CUDA(cudaStreamSynchronize(m->stream));
+      memcpy(&A.hz_max, &bits, sizeof(float));
+    }
   }
   SDTFE_CUDA(cudaGetLastError());
   return DTFE_OK;
@@ -456,6 +505,7 @@ void mesh_drop_records(Mesh* m, int axis) {
   if (m->stream) cudaStreamSynchronize(m->stream);
   dfree(m->ax[axis].rec64, m->nt, m);
   dfree(m->ax[axis].rec32, m->nt, m);
+  dfree(m->ax[axis].rot32, 4 * (size_t)m->nt, m);
 }
 
 dtfe_status_t mesh_hull_mask(Mesh* m, int axis, uint32_t* host_mask_out, int* count_out) {
@@ -570,6 +620,7 @@ void mesh_free(Mesh* m) {
   for (auto& A : m->ax) {
     dfree(A.rec64, m->nt, m);
     dfree(A.rec32, m->nt, m);
+    dfree(A.rot32, 4 * (size_t)m->nt, m);
     dfree(A.tri, A.n_tri, m);
     dfree(A.tri_rows, 8 * (size_t)A.n_tri, m);
   }

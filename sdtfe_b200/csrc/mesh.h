@@ -54,6 +54,8 @@ struct AxisData {
   // walk records in this axis' projected frame (built on demand, per precision)
   TetRec64* rec64 = nullptr;
   TetRec32* rec32 = nullptr;
+  TetRot32* rot32 = nullptr;  // 4 per tet (one per entry face), with rec32
+  float hz_max = 0.f;         // largest z extent of a tet in this frame
 };
 
 struct Mesh {

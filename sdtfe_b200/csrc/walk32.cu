@@ -57,6 +57,11 @@ struct MixConf {
   int max_visits;
   const TetRec64* __restrict__ rec64;  // exact coordinates when the floats are not
   int exact32;                         // the float coordinates are the doubles
+  const TetRot32* __restrict__ rot;    // records per entry face (NULL: general steps only)
+  const TetRec32* __restrict__ rec32;  // the mesh-order records
+  // Chord midpoints inside (zlo_in, zhi_in) are surely inside the slab for
+  // every tet of the mesh; others are tested against their own error bound.
+  double zlo_in, zhi_in;
 };
 
 struct RayState {
@@ -314,10 +319,11 @@ __device__ __noinline__ double midpoint64(const TetRec32* __restrict__ R32,
 __device__ __forceinline__ double chord32(const TetRec32* __restrict__ R, const MixConf& C,
                                           const RayState& r, int t, int enter, int leave,
                                           double z_in, float f_in, double z_out, float f_out,
-                                          float hz, int* fallbacks) {
+                                          float hz, float e_inout, int* fallbacks) {
   const double d = z_out - z_in;
   const float zm = (float)(z_in + 0.5 * d);
-  const float guard = 64.f * kEps * (fabsf(zm) + hz);
+  // float rounding of the midpoint plus the crossings' own error bounds
+  const float guard = 64.f * kEps * (fabsf(zm) + hz) + e_inout;
   bool inside;
   if (fabsf(zm - C.z0) > guard && fabsf(zm - C.z1) > guard) {
     inside = zm > C.z0 && zm < C.z1;
@@ -329,8 +335,255 @@ __device__ __forceinline__ double chord32(const TetRec32* __restrict__ R, const 
   return inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
 }
 
+// Fast-step table: for entry face F and the sign bits of the rotated products
+// (e01, e12, e20, a0, a1, a2 = u(0,1), u(1,2), u(2,0), u(3,0), u(3,1), u(3,2)),
+// the rotated slot k (0..2) whose opposite face the ray leaves through, with
+// bit 2 set, when the reference's rule (face_lut_entry on the products in the
+// mesh's own edge order) enters through F; 0 otherwise.  A product of a
+// reversed edge is the exact negative (the reference's formula is
+// antisymmetric in its two vertices), so the mesh-order signs follow from the
+// rotated ones.
+__host__ __device__ constexpr unsigned rot_lut_entry(int F, unsigned neg_rot) {
+  // rotated pair (p, q) -> product index j and reversal
+  unsigned neg = 0;
+  for (int e = 0; e < 6; ++e) {
+    constexpr int P[6] = {2, 2, 1, 2, 1, 3}, Q[6] = {1, 0, 0, 3, 3, 0};  // kEdgeP / kEdgeQ
+    const int p = rot_inv(F, P[e]), q = rot_inv(F, Q[e]);
+    int j = 0;
+    bool rev = false;
+    if (p == 3 || q == 3) {  // apex edge: a_k = u(3, k)
+      j = 3 + (p == 3 ? q : p);
+      rev = q == 3;
+    } else if ((p + 1) % 3 == q) {  // face edge in cyclic order: u(0,1), u(1,2), u(2,0)
+      j = p;
+    } else {
+      j = q;
+      rev = true;
+    }
+    neg |= (((neg_rot >> j) & 1u) ^ (rev ? 1u : 0u)) << e;
+  }
+  const unsigned ent = face_lut_entry(neg);
+  if (!(ent & 16u)) return 0u;
+  const int enter = (int)(ent & 3u), leave = (int)((ent >> 2) & 3u);
+  if (enter != F || leave == F) return 0u;
+  return (unsigned)rot_inv(F, leave) | 4u;
+}
+
+template <class T>
+__device__ __forceinline__ T sel3(int k, T a, T b, T c) {
+  return k == 0 ? a : (k == 1 ? b : c);
+}
+
+struct FastStep {
+  double z_out;    // exit crossing
+  double contrib;  // the chord's share of the integral
+  float f_out;     // field at the exit crossing
+  float e_out;     // bound on the exit crossing's z error
+  int next;        // record of the next tet
+};
+
+// One walk step on the record of (tet, entry face), for a ray whose entry
+// crossing (z_in, f_in) was carried over from the previous tet.  Succeeds
+// when the FP32 products decide all six reference signs, the reference's rule
+// enters through the known face and the chord midpoint is clear of the slab
+// bounds; otherwise nothing is committed and the general step takes the tet.
+// The exit crossing is FP32 unless it is ill-conditioned or on the hull, where
+// it is the exact one (o->next = -1: the ray leaves the mesh here).
+__device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, int ri,
+                                          const unsigned char* __restrict__ lut4, double z_in,
+                                          float f_in, float e_in, FastStep* o, int* fallbacks) {
+  const TetRot32* p = C.rot + ri;
+  const float4 a = __ldg(&p->xy01), b = __ldg(&p->xy23), z = __ldg(&p->z), f = __ldg(&p->fld);
+  const int4 nb = __ldg(&p->nb);
+  const float x0 = __fsub_rn(__fsub_rn(a.x, r.oxh), r.oxl), y0 = __fsub_rn(__fsub_rn(a.y, r.oyh), r.oyl);
+  const float x1 = __fsub_rn(__fsub_rn(a.z, r.oxh), r.oxl), y1 = __fsub_rn(__fsub_rn(a.w, r.oyh), r.oyl);
+  const float x2 = __fsub_rn(__fsub_rn(b.x, r.oxh), r.oxl), y2 = __fsub_rn(__fsub_rn(b.y, r.oyh), r.oyl);
+  const float x3 = __fsub_rn(__fsub_rn(b.z, r.oxh), r.oxl), y3 = __fsub_rn(__fsub_rn(b.w, r.oyh), r.oyl);
+  const float dmax = fmaxf(fmaxf(fmaxf(fabsf(x0), fabsf(y0)), fmaxf(fabsf(x1), fabsf(y1))),
+                           fmaxf(fmaxf(fabsf(x2), fabsf(y2)), fmaxf(fabsf(x3), fabsf(y3))));
+  // the bound of tet_test: FP32 and reference rounding plus the threshold
+  const float bound = __fmaf_ru(48.f * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
+  const float e01 = __fmaf_rn(x0, y1, -__fmul_rn(y0, x1));
+  const float e12 = __fmaf_rn(x1, y2, -__fmul_rn(y1, x2));
+  const float e20 = __fmaf_rn(x2, y0, -__fmul_rn(y2, x0));
+  const float a0 = __fmaf_rn(x3, y0, -__fmul_rn(y3, x0));
+  const float a1 = __fmaf_rn(x3, y1, -__fmul_rn(y3, x1));
+  const float a2 = __fmaf_rn(x3, y2, -__fmul_rn(y3, x2));
+  const float umin = fminf(fminf(fminf(fabsf(e01), fabsf(e12)), fminf(fabsf(e20), fabsf(a0))),
+                           fminf(fabsf(a1), fabsf(a2)));
+  if (!(umin > bound)) return false;
+  const unsigned neg = (__float_as_uint(e01) >> 31) | ((__float_as_uint(e12) >> 31) << 1) |
+                       ((__float_as_uint(e20) >> 31) << 2) | ((__float_as_uint(a0) >> 31) << 3) |
+                       ((__float_as_uint(a1) >> 31) << 4) | ((__float_as_uint(a2) >> 31) << 5);
+  const unsigned code = lut4[((unsigned)(ri & 3) << 6) | neg];
+  if (!(code & 4u)) return false;
+  const int k = (int)(code & 3u);
+  const int next = sel3(k, nb.x, nb.y, nb.z);
+  if (next < -1) return false;  // a neighbour that does not list this tet
+  // exit face: apex (slot 3) and slots i = k+1, j = k+2 (mod 3); the weight of
+  // each corner is the product of the face edge opposite it
+  const float w3 = sel3(k, e12, e20, e01);
+  const float wi = -sel3(k, a2, a0, a1);
+  const float wj = sel3(k, a1, a2, a0);
+  const float zi = sel3(k, z.y, z.z, z.x), zj = sel3(k, z.z, z.x, z.y);
+  const float fi = sel3(k, f.y, f.z, f.x), fj = sel3(k, f.z, f.x, f.y);
+  const float den = w3 + wi + wj;
+  const float rr = __fdividef(1.f, den);
+  const float cond = 3.f * bound * fabsf(rr);  // relative error of the weights
+  const float hi = zi - z.w, hj = zj - z.w;
+  double z_out;
+  float f_out, e_out;
+  if (next == -1 || !(cond <= kCrossingTol)) {  // not shared, or ill-conditioned: exact
+    const double2 c = exact_crossing(C.rec32, C.rec64, C.exact32, C.lz, ri >> 2,
+                                     rot_slot(ri & 3, k), r.ox, r.oy);
+    z_out = c.x;
+    f_out = (float)c.y;
+    e_out = 0.f;
+    ++*fallbacks;
+  } else {
+    const float dzr = rr * __fmaf_rn(wj, hj, wi * hi);
+    f_out = rr * __fmaf_rn(wj, fj, __fmaf_rn(wi, fi, w3 * f.w));
+    // z error: the weights' error over the face's height above the apex, plus
+    // the rounding of the offset (the double sum with the apex z is exact)
+    e_out = (cond + 8.f * kEps) * fmaxf(fabsf(hi), fabsf(hj));
+    z_out = (double)z.w + (double)dzr;
+  }
+  const double d = z_out - z_in;
+  const double zm = z_in + 0.5 * d;
+  bool inside = true;
+  if (!(zm > C.zlo_in && zm < C.zhi_in)) {  // near a slab bound: this chord's own guard
+    const float g = 64.f * kEps * fabsf((float)zm) + e_in + e_out;
+    const float d0 = (float)(zm - C.z0d), d1 = (float)(zm - C.z1d);
+    if (!(fabsf(d0) > g && fabsf(d1) > g)) return false;  // the reference's midpoint decides
+    inside = d0 > 0.f && d1 < 0.f;
+  }
+  o->z_out = z_out;
+  o->f_out = f_out;
+  o->e_out = e_out;
+  o->contrib = inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
+  o->next = next;
+  return true;
+}
+
+// Record of the neighbour across face m of tet t, as entered from t (-1: none).
+__device__ __forceinline__ int rot_next(const MixConf& C, int t, int m) {
+  if (!C.rot) return -1;
+  const int G = m == 0 ? 1 : 0;  // a record of t whose entry face is not m
+  const int4 nb = __ldg(&C.rot[4 * (size_t)t + G].nb);
+  const int v = sel3(rot_inv(G, m), nb.x, nb.y, nb.z);
+  return v >= 0 ? v : -1;
+}
+
+// State of one ray between steps.
+struct WalkState {
+  RayState r;
+  double sum, z_in;
+  float f_in, e_in;  // e_in: bound on z_in's error
+  uint64_t ctr;      // perturbation draws so far
+  int crossed, fallbacks, cur, prev, ri;
+  bool carried;      // z_in / f_in hold the crossing of the face shared with prev
+};
+
+constexpr int kWalkOn = -1;  // general_step: the walk continues
+
+// The general step on tet w.cur (src/dtfe.c:300-372): the mesh-order record,
+// the filtered test with the reference's FP64 signs as fallback, perturbation,
+// the chord, and the move through the leave face, or through the enter face
+// when the leave face leads back to the previous tet (the reference's
+// turn-around).  The crossing of the face passed through is carried on.
+// Returns kWalkOn, or the ray's final status.  Kept out of line: it runs on
+// about one step in a hundred and would otherwise crowd the fast loop's
+// registers.
+__device__ __noinline__ int general_step(const TetRec32* __restrict__ R, const MixConf& C,
+                                         uint64_t ray, const unsigned char* __restrict__ lut,
+                                         WalkState& w, int* visits, int max_record) {
+  RayState& r = w.r;
+  const int cur = w.cur;
+  int4 nb;
+  Verts32 v;
+  load32(R, cur, v, nb);
+  float u[6], bmax;
+  Hit32 h = tet_test(R, C, r, cur, v, u, &bmax, lut, &w.fallbacks);
+  if (!h.ok) return kRayNoExit;
+  int np = 0;
+  while (h.special) {  // FP64 perturbation, exactly as the reference (src/dtfe.c:219-245)
+    const int k = sdtfe_rand31(C.seed, ray, w.ctr++) % 4;
+    const double2 vk = xy64_at(R, C.rec64, C.exact32, cur, k);
+    double dx = __dsub_rn(vk.x, r.ox);
+    double dy = __dsub_rn(vk.y, r.oy);
+    const double mag = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+    if (mag > C.dist) {
+      dx = __ddiv_rn(dx, mag);
+      dy = __ddiv_rn(dy, mag);
+      dx = __dmul_rn(dx, C.dist);
+      dy = __dmul_rn(dy, C.dist);
+    }
+    r.ox = __dadd_rn(r.ox, dx);
+    r.oy = __dadd_rn(r.oy, dy);
+    ray_setup(r, C);
+    w.carried = false;  // the ray moved: this tet computes its own entry
+    if (++np > kPerturbMax) return kRayPerturbMax;
+    h = tet_test(R, C, r, cur, v, u, &bmax, lut, &w.fallbacks);
+    if (!h.ok) return kRayNoExit;
+  }
+  const int enter = h.enter, leave = h.leave;
+  if (visits != nullptr && w.crossed < max_record) visits[w.crossed] = cur;
+  ++w.crossed;
+
+  // entry crossing: carried over from the previous chord, or computed from
+  // the exact operands where it is not shared (first tet, perturbation,
+  // turn-around)
+  if (!w.carried || nb_at(nb, enter) != w.prev) {
+    const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, enter, r.ox, r.oy);
+    w.z_in = c.x;
+    w.f_in = (float)c.y;
+    w.e_in = 0.f;
+    ++w.fallbacks;
+  }
+  // exit crossing: FP32 unless it leaves the mesh (not shared with a
+  // neighbouring chord) or is ill-conditioned
+  float dzo, f_out, e_out = 0.f;
+  double z_out;
+  const float cond = crossing(leave, u, bmax, v, &dzo, &f_out);
+  const float hz = fmaxf(fmaxf(fabsf(v.z[1] - v.z[0]), fabsf(v.z[2] - v.z[0])),
+                         fabsf(v.z[3] - v.z[0]));
+  if (nb_at(nb, leave) == -1 || !(cond <= kCrossingTol)) {
+    const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
+    z_out = c.x;
+    f_out = (float)c.y;
+    ++w.fallbacks;
+  } else {
+    z_out = (double)v.z[0] + (double)dzo;
+    e_out = (cond + 8.f * kEps) * hz;
+  }
+  w.sum += chord32(R, C, r, cur, enter, leave, w.z_in, w.f_in, z_out, f_out, hz, w.e_in + e_out,
+                   &w.fallbacks);
+
+  // move on (src/dtfe.c:300-309)
+  int m = leave;
+  int nx = nb_at(nb, leave);
+  if (nx == w.prev) {
+    m = enter;
+    nx = nb_at(nb, enter);
+  }
+  if (nx == -1) return kRayOk;
+  if (m == leave) {
+    w.z_in = z_out;
+    w.f_in = f_out;
+    w.e_in = e_out;
+  }  // else the enter face's crossing, already in z_in
+  w.carried = true;
+  w.ri = rot_next(C, cur, m);
+  w.prev = cur;
+  w.cur = nx;
+  return kWalkOn;
+}
+
 // The mixed walk.  Same control flow as walk64 (src/dtfe.c:247-374); returns
-// the status, the integral in *rho and the crossing count.
+// the status, the integral in *rho and the crossing count.  A tet entered
+// through a face shared with the previous one (the crossing there carried
+// over) takes the fast step on its record for that entry face; the first
+// tet, and any tet the fast step declines, takes the general step.
 __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixConf& C, int ft,
                                       double x, double y, uint64_t ray,
                                       const unsigned char* __restrict__ lut, double* rho_out,
@@ -346,105 +599,77 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
   ray_setup(r, C);
   uint64_t ctr = 0;
   double sum = 0.0, z_in = 0.0;
-  float f_in = 0.f;
-  bool carried = false;  // z_in / f_in hold the previous tet's exit crossing
+  float f_in = 0.f, e_in = 0.f;
+  bool carried = false;
   int crossed = 0, fallbacks = 0;
-  int4 nb = make_int4(ft, -1, -1, -1);
-  int leave = 0, enter = -1;
   int cur = ft, prev = -1;
+  int ri = -1;  // cur's record for its entry face (-1: general step)
+  int status = kWalkOn;
   for (;;) {
-    int nx = nb_at(nb, leave);
-    if (nx == -1) break;
-    if (nx == prev) {
-      const int t = enter;
-      enter = leave;
-      leave = t;
-      nx = nb_at(nb, leave);
-      if (nx == -1) break;
-    }
-    prev = cur;
-    cur = nx;
     if (crossed >= C.max_visits) {
-      *fallbacks_out = fallbacks;
-      return kRayBudget;
+      status = kRayBudget;
+      break;
     }
-    Verts32 v;
-    load32(R, cur, v, nb);
-    float u[6], bmax;
-    Hit32 h = tet_test(R, C, r, cur, v, u, &bmax, lut, &fallbacks);
-    if (!h.ok) {
-      *fallbacks_out = fallbacks;
-      return kRayNoExit;
-    }
-    int np = 0;
-    while (h.special) {  // FP64 perturbation, exactly as the reference (src/dtfe.c:219-245)
-      const int k = sdtfe_rand31(C.seed, ray, ctr++) % 4;
-      const double2 vk = xy64_at(R, C.rec64, C.exact32, cur, k);
-      double dx = __dsub_rn(vk.x, r.ox);
-      double dy = __dsub_rn(vk.y, r.oy);
-      const double mag = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-      if (mag > C.dist) {
-        dx = __ddiv_rn(dx, mag);
-        dy = __ddiv_rn(dy, mag);
-        dx = __dmul_rn(dx, C.dist);
-        dy = __dmul_rn(dy, C.dist);
-      }
-      r.ox = __dadd_rn(r.ox, dx);
-      r.oy = __dadd_rn(r.oy, dy);
-      ray_setup(r, C);
-      carried = false;  // the ray moved: this tet computes its own entry
-      if (++np > kPerturbMax) {
-        *fallbacks_out = fallbacks;
-        return kRayPerturbMax;
-      }
-      h = tet_test(R, C, r, cur, v, u, &bmax, lut, &fallbacks);
-      if (!h.ok) {
-        *fallbacks_out = fallbacks;
-        return kRayNoExit;
+    if (ri >= 0) {
+      FastStep o;
+      if (fast_step(C, r, ri, lut + 64, z_in, f_in, e_in, &o, &fallbacks)) {
+        if (visits != nullptr && crossed < max_record) visits[crossed] = cur;
+        ++crossed;
+        sum += o.contrib;
+        if (o.next < 0) {  // left the mesh
+          status = kRayOk;
+          break;
+        }
+        z_in = o.z_out;
+        f_in = o.f_out;
+        e_in = o.e_out;
+        prev = cur;
+        ri = o.next;
+        cur = ri >> 2;
+        continue;
       }
     }
-    enter = h.enter;
-    leave = h.leave;
-    if (visits != nullptr && crossed < max_record) visits[crossed] = cur;
-    ++crossed;
-
-    // entry crossing: carried over from the previous chord, or computed from
-    // the exact operands where it is not shared (first tet, perturbation,
-    // turn-around)
-    if (!carried || nb_at(nb, enter) != prev) {
-      const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, enter, r.ox, r.oy);
-      z_in = c.x;
-      f_in = (float)c.y;
-      ++fallbacks;
-    }
-    // exit crossing: FP32 unless it leaves the mesh (not shared with a
-    // neighbouring chord) or is ill-conditioned
-    float dzo, f_out;
-    double z_out;
-    const float cond = crossing(leave, u, bmax, v, &dzo, &f_out);
-    if (nb_at(nb, leave) == -1 || !(cond <= kCrossingTol)) {
-      const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
-      z_out = c.x;
-      f_out = (float)c.y;
-      ++fallbacks;
-    } else {
-      z_out = (double)v.z[0] + (double)dzo;
-    }
-    const float hz = fmaxf(fmaxf(fabsf(v.z[1] - v.z[0]), fabsf(v.z[2] - v.z[0])),
-                           fabsf(v.z[3] - v.z[0]));
-    sum += chord32(R, C, r, cur, enter, leave, z_in, f_in, z_out, f_out, hz, &fallbacks);
-    z_in = z_out;
-    f_in = f_out;
-    carried = true;
+    WalkState w;
+    w.r = r;
+    w.sum = sum;
+    w.z_in = z_in;
+    w.f_in = f_in;
+    w.e_in = e_in;
+    w.ctr = ctr;
+    w.crossed = crossed;
+    w.fallbacks = fallbacks;
+    w.cur = cur;
+    w.prev = prev;
+    w.ri = -1;
+    w.carried = carried;
+    status = general_step(R, C, ray, lut, w, visits, max_record);
+    r = w.r;
+    sum = w.sum;
+    z_in = w.z_in;
+    f_in = w.f_in;
+    e_in = w.e_in;
+    ctr = w.ctr;
+    crossed = w.crossed;
+    fallbacks = w.fallbacks;
+    cur = w.cur;
+    prev = w.prev;
+    ri = w.ri;
+    carried = w.carried;
+    if (status != kWalkOn) break;
   }
   *crossed_out = crossed;
-  *rho_out = sum;
+  *rho_out = status == kRayOk ? sum : 0.0;
   *fallbacks_out = fallbacks;
-  return kRayOk;
+  return status;
 }
 
+// Shared-memory tables of the walk: the face rule on 64 sign patterns, then
+// the fast-step table (256 entries).
+constexpr int kLutBytes = 64 + 256;
+
 __device__ __forceinline__ void fill_lut(unsigned char* lut) {
-  for (int i = threadIdx.x; i < 64; i += blockDim.x) lut[i] = (unsigned char)face_lut_entry(i);
+  for (int i = threadIdx.x; i < kLutBytes; i += blockDim.x)
+    lut[i] = (unsigned char)(i < 64 ? face_lut_entry(i) : rot_lut_entry((i - 64) >> 6, (i - 64) & 63u));
 }
 
 struct MapArgs32 {
@@ -545,9 +770,9 @@ __device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
 // register budget) are compile-time; the autotuner picks among the
 // instantiations.
 template <int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_map32(const MapArgs32 a) {
+__global__ void __launch_bounds__(BLOCK, MINB) k_map32(const __grid_constant__ MapArgs32 a) {
   extern __shared__ double s_val32[];  // P*S doubles, then P*S success bytes
-  __shared__ unsigned char s_lut[64];
+  __shared__ unsigned char s_lut[kLutBytes];
   fill_lut(s_lut);
   __syncthreads();
   unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + a.TW * a.TH * a.S);
@@ -564,7 +789,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
     k_batch32(const BatchJob32* __restrict__ jobs, int n_jobs, long long total_tiles,
               unsigned long long* __restrict__ queue) {
   extern __shared__ double s_val32[];
-  __shared__ unsigned char s_lut[64];
+  __shared__ unsigned char s_lut[kLutBytes];
   __shared__ MapArgs32 s_args;
   __shared__ long long s_tile;
   __shared__ int s_job;
@@ -602,12 +827,13 @@ __global__ void __launch_bounds__(BLOCK, MINB)
 __global__ void __launch_bounds__(128) k_trace32(const TetRec32* __restrict__ rec,
                                                  const TriRec64* __restrict__ tri, int n_tri,
                                                  int n_rays, const double* __restrict__ xs,
-                                                 const double* __restrict__ ys, MixConf C,
+                                                 const double* __restrict__ ys,
+                                                 const __grid_constant__ MixConf C,
                                                  int loc_budget, double* __restrict__ rho,
                                                  int* __restrict__ crossed,
                                                  int* __restrict__ status,
                                                  int* __restrict__ visits, int max_record) {
-  __shared__ unsigned char s_lut[64];
+  __shared__ unsigned char s_lut[kLutBytes];
   fill_lut(s_lut);
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -639,6 +865,16 @@ MixConf mix_conf(const Mesh& m, int axis, double z0, double lz, double dist, uin
   C.max_visits = max_visits;
   C.rec64 = m.ax[axis].rec64;
   C.exact32 = m.fp32_exact ? 1 : 0;
+  C.rot = m.ax[axis].rot32;
+  C.rec32 = m.ax[axis].rec32;
+  // A midpoint from FP32-derived crossings is within tol * H of the
+  // reference's (each crossing within tol times its tet's height, H the
+  // largest) plus float rounding of positions of magnitude up to Z.
+  const double H = m.ax[axis].hz_max;
+  const double Z = fmax(fmax(fabs(C.z0d), fabs(C.z1d)), m.coord_max);
+  const double G = 64.0 * 5.9604644775390625e-08 * (Z + H) + 2.0 * (double)kCrossingTol * H;
+  C.zlo_in = C.z0d + G;
+  C.zhi_in = C.z1d - G;
   return C;
 }
 

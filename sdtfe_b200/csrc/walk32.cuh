@@ -1,11 +1,12 @@
-// walk32.cuh - record layout of the mixed-precision walk.
+// walk32.cuh - record layouts of the mixed-precision walk.
 #pragma once
 
 #include <cstdint>
 
 namespace sdtfe {
 
-// 96 B per tet: everything one FP32 walk step reads, in six 16-byte words.
+// 96 B per tet: everything one FP32 walk step reads, in six 16-byte words,
+// vertices in the mesh's own order (A..D).  The general step reads these.
 struct __align__(32) TetRec32 {
   float4 xyab;  // (x_A, y_A, x_B, y_B) in the projected frame
   float4 xycd;  // (x_C, y_C, x_D, y_D)
@@ -15,5 +16,28 @@ struct __align__(32) TetRec32 {
   int4 aux;     // vertex ids A..D
 };
 static_assert(sizeof(TetRec32) == 96, "TetRec32 layout");
+
+// 80 B per (tet, entry face): the tet seen by a ray that entered it through
+// face F.  Slots 0..2 hold face F's vertices (in the order the face is listed
+// in: BDC, ACD, ADB, ABC), slot 3 the vertex opposite it.  Record 4*t + F.
+// The fast step reads one of these: the entry face is known, so every slot
+// is fixed and only the exit face (opposite slot 0, 1 or 2) is chosen.
+struct __align__(16) TetRot32 {
+  float4 xy01;  // (x0, y0, x1, y1)
+  float4 xy23;  // (x2, y2, x3, y3)
+  float4 z;     // (z0, z1, z2, z3)
+  float4 fld;   // (rho0, rho1, rho2, rho3)
+  int4 nb;      // x..z: record 4*n + F' of the neighbour n across the face opposite
+                // slot 0..2, F' the face of n shared with this tet; -1 on the hull,
+                // INT_MIN when n does not list this tet; w: the tet id
+};
+static_assert(sizeof(TetRot32) == 80, "TetRot32 layout");
+
+// Original vertex slot of rotated slot k for entry face F, and its inverse;
+// two bits per entry, one byte per F.
+constexpr uint32_t kRotSlots = 0xE49C782Du;
+constexpr uint32_t kRotInverse = 0xE4789C63u;
+__host__ __device__ constexpr int rot_slot(int F, int k) { return (int)((kRotSlots >> (8 * F + 2 * k)) & 3u); }
+__host__ __device__ constexpr int rot_inv(int F, int v) { return (int)((kRotInverse >> (8 * F + 2 * v)) & 3u); }
 
 }  // namespace sdtfe
