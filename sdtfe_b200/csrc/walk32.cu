@@ -45,6 +45,15 @@ namespace {
 
 constexpr float kEps = 5.9604645e-08f;  // 2^-24, FP32 unit roundoff
 
+// Error of one FP32 product u = px*qy - py*qx of relative coordinates, in
+// units of kEps * dmax^2 (dmax: the tet's largest |relative coordinate|).
+// Each relative coordinate (v - o_hi) - o_lo is within 2 kEps dmax (+ a term
+// in kEps^2 |o| that e_coef covers) of v - o, which moves the product by at
+// most 4 * 2 kEps dmax^2; rounding the product adds at most 4 kEps dmax^2
+// (two products and a difference, each rounded once; 3 with a fused
+// multiply-add).  16 covers the 12 with a margin.
+constexpr float kProdErr = 16.f;
+
 struct MixConf {
   double lz;          // slab depth (the reference's ray length)
   double z0d, z1d;    // slab bounds
@@ -74,9 +83,10 @@ struct RayState {
 // Float hi/lo split of the origin and this ray's filter constants.  The
 // reference's own FP64 error on a product is at most 8 roundings of
 // magnitude <= 6*M^2*lz (M: largest coordinate or origin magnitude), i.e.
-// 48*2^-53*M^2 in units of lz.  A relative coordinate carries at most
-// 3*eps^2*|o| from the split plus the records' rounding (e_abs); on a product
-// that is at most 2*e_abs*(|px|+|py|+|qx|+|qy|) <= 8*e_abs*Dmax.
+// 48*2^-53*M^2 in units of lz.  Beyond the relative error of the
+// subtractions (kProdErr), a relative coordinate carries at most 3*eps^2*|o|
+// from the split plus the records' rounding (e_abs); on a product that is at
+// most 2*e_abs*(|px|+|py|+|qx|+|qy|) <= 8*e_abs*Dmax.
 __device__ __forceinline__ void ray_setup(RayState& r, const MixConf& C) {
   r.oxh = (float)r.ox;
   r.oxl = (float)(r.ox - (double)r.oxh);
@@ -198,10 +208,10 @@ __device__ __forceinline__ Hit32 tet_test(const TetRec32* __restrict__ R32, cons
     dy[k] = __fsub_rn(__fsub_rn(v.y[k], r.oyh), r.oyl);
     dmax = fmaxf(dmax, fmaxf(fabsf(dx[k]), fabsf(dy[k])));
   }
-  // one bound for the tet's six products: |ue - u'| <= 6 eps (|a| + |b|)
-  // + 2 e_abs sum|d| with |a|, |b| <= dmax^2; 48 eps dmax^2 is 4x the first
-  // term, e_coef dmax covers the second, thr_hi is the reference's threshold
-  const float bound = __fmaf_ru(48.f * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
+  // one bound for the tet's six products: the FP32 error (kProdErr), the
+  // records' rounding and the origin split (e_coef), and the reference's
+  // threshold plus its own FP64 rounding (thr_hi)
+  const float bound = __fmaf_ru(kProdErr * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
   unsigned neg = 0, unc = 0;
 #pragma unroll
   for (int e = 0; e < 6; ++e) {
@@ -379,7 +389,7 @@ struct FastStep {
   double contrib;  // the chord's share of the integral
   float f_out;     // field at the exit crossing
   float e_out;     // bound on the exit crossing's z error
-  int next;        // record of the next tet
+  int next;        // record of the next tet; -1: the ray left the mesh here
 };
 
 // One walk step on the record of (tet, entry face), for a ray whose entry
@@ -387,11 +397,14 @@ struct FastStep {
 // when the FP32 products decide all six reference signs, the reference's rule
 // enters through the known face and the chord midpoint is clear of the slab
 // bounds; otherwise nothing is committed and the general step takes the tet.
-// The exit crossing is FP32 unless it is ill-conditioned or on the hull, where
-// it is the exact one (o->next = -1: the ray leaves the mesh here).
+// The step also declines an ill-conditioned exit crossing, and an exit
+// through the hull (o->next = -1 on success) unless the error its FP32
+// crossing can add to the chord is below 1e-7 of the ray's integral (sum):
+// such a crossing is not shared with a neighbouring chord, so its error does
+// not cancel.  The general step computes those crossings exactly.
 __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, int ri,
                                           const unsigned char* __restrict__ lut4, double z_in,
-                                          float f_in, float e_in, FastStep* o, int* fallbacks) {
+                                          float f_in, float e_in, double sum, FastStep* o) {
   const TetRot32* p = C.rot + ri;
   const float4 a = __ldg(&p->xy01), b = __ldg(&p->xy23), z = __ldg(&p->z), f = __ldg(&p->fld);
   const int4 nb = __ldg(&p->nb);
@@ -402,7 +415,7 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   const float dmax = fmaxf(fmaxf(fmaxf(fabsf(x0), fabsf(y0)), fmaxf(fabsf(x1), fabsf(y1))),
                            fmaxf(fmaxf(fabsf(x2), fabsf(y2)), fmaxf(fabsf(x3), fabsf(y3))));
   // the bound of tet_test: FP32 and reference rounding plus the threshold
-  const float bound = __fmaf_ru(48.f * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
+  const float bound = __fmaf_ru(kProdErr * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
   const float e01 = __fmaf_rn(x0, y1, -__fmul_rn(y0, x1));
   const float e12 = __fmaf_rn(x1, y2, -__fmul_rn(y1, x2));
   const float e20 = __fmaf_rn(x2, y0, -__fmul_rn(y2, x0));
@@ -431,23 +444,13 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   const float rr = __fdividef(1.f, den);
   const float cond = 3.f * bound * fabsf(rr);  // relative error of the weights
   const float hi = zi - z.w, hj = zj - z.w;
-  double z_out;
-  float f_out, e_out;
-  if (next == -1 || !(cond <= kCrossingTol)) {  // not shared, or ill-conditioned: exact
-    const double2 c = exact_crossing(C.rec32, C.rec64, C.exact32, C.lz, ri >> 2,
-                                     rot_slot(ri & 3, k), r.ox, r.oy);
-    z_out = c.x;
-    f_out = (float)c.y;
-    e_out = 0.f;
-    ++*fallbacks;
-  } else {
-    const float dzr = rr * __fmaf_rn(wj, hj, wi * hi);
-    f_out = rr * __fmaf_rn(wj, fj, __fmaf_rn(wi, fi, w3 * f.w));
-    // z error: the weights' error over the face's height above the apex, plus
-    // the rounding of the offset (the double sum with the apex z is exact)
-    e_out = (cond + 8.f * kEps) * fmaxf(fabsf(hi), fabsf(hj));
-    z_out = (double)z.w + (double)dzr;
-  }
+  if (!(cond <= kCrossingTol)) return false;  // ill-conditioned
+  const float dzr = rr * __fmaf_rn(wj, hj, wi * hi);
+  const float f_out = rr * __fmaf_rn(wj, fj, __fmaf_rn(wi, fi, w3 * f.w));
+  // z error: the weights' error over the face's height above the apex, plus
+  // the rounding of the offset (the double sum with the apex z is exact)
+  const float e_out = (cond + 8.f * kEps) * fmaxf(fabsf(hi), fabsf(hj));
+  const double z_out = (double)z.w + (double)dzr;
   const double d = z_out - z_in;
   const double zm = z_in + 0.5 * d;
   bool inside = true;
@@ -457,10 +460,18 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
     if (!(fabsf(d0) > g && fabsf(d1) > g)) return false;  // the reference's midpoint decides
     inside = d0 > 0.f && d1 < 0.f;
   }
+  const double contrib = inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
+  if (next == -1 && inside) {
+    // what the FP32 exit can add: its field error (the weights' error over
+    // the face's largest vertex value) over half the chord, and its z error
+    const float e_f = (cond + 8.f * kEps) * fmaxf(fmaxf(fabsf(fi), fabsf(fj)), fabsf(f.w));
+    const float e_c = 0.5f * (e_f * fabsf((float)d) + fabsf(f_in + f_out) * e_out);
+    if (!(e_c <= 1e-7f * (float)fabs(sum + contrib))) return false;
+  }
   o->z_out = z_out;
   o->f_out = f_out;
   o->e_out = e_out;
-  o->contrib = inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
+  o->contrib = contrib;
   o->next = next;
   return true;
 }
@@ -612,7 +623,7 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
     }
     if (ri >= 0) {
       FastStep o;
-      if (fast_step(C, r, ri, lut + 64, z_in, f_in, e_in, &o, &fallbacks)) {
+      if (fast_step(C, r, ri, lut + 64, z_in, f_in, e_in, sum, &o)) {
         if (visits != nullptr && crossed < max_record) visits[crossed] = cur;
         ++crossed;
         sum += o.contrib;
