@@ -695,10 +695,14 @@ def run_ours(args, pre=None):
                    "sample": f"unavailable: {e}"}
 
     extra = {}
-    if sections and "batch" in sections:
-        extra["batch"] = section_batch(args, sd, torch, dev, stream, flush, tri)
-    if sections and "serving" in sections:
-        extra["serving"] = section_serving(args, sd, torch, tri)
+    for name, fn in (("batch", lambda: section_batch(args, sd, torch, dev, stream, flush, tri)),
+                     ("serving", lambda: section_serving(args, sd, torch, tri))):
+        if sections and name in sections:
+            try:
+                extra[name] = fn()
+            except Exception as e:  # a section must not cost the headline line
+                extra[name] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.synchronize()
     if qinfo:
         extra["qhull_pool"] = qinfo
 

@@ -206,6 +206,16 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
       nxt[s] = f >= 0 ? 4 * n + f : INT_MIN;
     }
     atomicMax(hz_bits, __float_as_int(zmax - zmin));  // non-negative: int order = float order
+    // extent of the projection, over the float coordinates the walk reads
+    float lo[2] = {(float)q[0][0], (float)q[0][1]}, hi[2] = {lo[0], lo[1]};
+#pragma unroll
+    for (int s = 1; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        lo[c] = fminf(lo[c], (float)q[s][c]);
+        hi[c] = fmaxf(hi[c], (float)q[s][c]);
+      }
+    const float ext = __fmul_ru(fmaxf(__fsub_ru(hi[0], lo[0]), __fsub_ru(hi[1], lo[1])), 1.0000010f);
 #pragma unroll
     for (int F = 0; F < 4; ++F) {
       const int s0 = rot_slot(F, 0), s1 = rot_slot(F, 1), s2 = rot_slot(F, 2), s3 = rot_slot(F, 3);
@@ -214,7 +224,7 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
       r.xy23 = make_float4((float)q[s2][0], (float)q[s2][1], (float)q[s3][0], (float)q[s3][1]);
       r.z = make_float4((float)q[s0][2], (float)q[s1][2], (float)q[s2][2], (float)q[s3][2]);
       r.fld = make_float4((float)p[s0].w, (float)p[s1].w, (float)p[s2].w, (float)p[s3].w);
-      r.nb = make_int4(nxt[s0], nxt[s1], nxt[s2], t);
+      r.nb = make_int4(nxt[s0], nxt[s1], nxt[s2], __float_as_int(ext));
       rot[4 * (size_t)t + F] = r;
     }
   }
@@ -471,32 +481,66 @@ dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32) {
   AxisData& A = m->ax[axis];
   const bool need64 = want64 && !A.rec64, need32 = want32 && !A.rec32;
   if (!need64 && !need32) return DTFE_OK;
-  if (need64) SDTFE_TRY(dmalloc(&A.rec64, m->nt, m));
   // rotated records address 4*t + F in an int: up to 2^29 - 1 tets
   const bool need_rot = need32 && m->nt < (1 << 29);
-  if (need32) SDTFE_TRY(dmalloc(&A.rec32, m->nt, m));
-  if (need_rot) SDTFE_TRY(dmalloc(&A.rot32, 4 * (size_t)m->nt, m));
-  if (m->nt) {
-    int* hz = nullptr;
+  // all or nothing: a record array that exists has been built
+  int* hz = nullptr;  // largest tet height, as float bits (non-negative: int order)
+  dtfe_status_t st = DTFE_OK;
+  if (need64) st = dmalloc(&A.rec64, m->nt, m);
+  if (st == DTFE_OK && need32) st = dmalloc(&A.rec32, m->nt, m);
+  if (st == DTFE_OK && need_rot) st = dmalloc(&A.rot32, 4 * (size_t)m->nt, m);
+  cudaError_t e = cudaSuccess;
+  int bits = 0;
+  if (st == DTFE_OK && m->nt) {
     if (need_rot) {
-      SDTFE_CUDA(cudaMallocAsync(&hz, sizeof(int), m->stream));
-      SDTFE_CUDA(cudaMemsetAsync(hz, 0, sizeof(int), m->stream));
+      e = cudaMallocAsync(&hz, sizeof(int), m->stream);
+      if (e == cudaSuccess) e = cudaMemsetAsync(hz, 0, sizeof(int), m->stream);
     }
-    k_records<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, axis,
-                                                         need64 ? A.rec64 : nullptr,
-                                                         need32 ? A.rec32 : nullptr,
-                                                         need_rot ? A.rot32 : nullptr, hz);
-    count_launch();
-    if (need_rot) {
-      int bits = 0;
-      SDTFE_CUDA(cudaMemcpyAsync(&bits, hz, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
-      cudaFreeAsync(hz, m->stream);
-      SDTFE_CUDA(cudaStreamSynchronize(m->stream));
-      memcpy(&A.hz_max, &bits, sizeof(float));
+    if (e == cudaSuccess) {
+      k_records<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, axis,
+                                                           need64 ? A.rec64 : nullptr,
+                                                           need32 ? A.rec32 : nullptr,
+                                                           need_rot ? A.rot32 : nullptr, hz);
+      count_launch();
+      e = cudaGetLastError();
     }
+    if (e == cudaSuccess && need_rot)
+      e = cudaMemcpyAsync(&bits, hz, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
+    if (hz) cudaFreeAsync(hz, m->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    if (e != cudaSuccess)
+      st = set_error(e == cudaErrorMemoryAllocation ? DTFE_ERR_NOMEM : DTFE_ERR_CUDA,
+                     "walk records: %s", cudaGetErrorString(e));
   }
+  if (st != DTFE_OK) {
+    if (need64) dfree(A.rec64, m->nt, m);
+    if (need32) dfree(A.rec32, m->nt, m);
+    if (need_rot) dfree(A.rot32, 4 * (size_t)m->nt, m);
+    return st;
+  }
+  if (need_rot) memcpy(&A.hz_max, &bits, sizeof(float));
   SDTFE_CUDA(cudaGetLastError());
   return DTFE_OK;
+}
+
+size_t mesh_record_bytes(const Mesh& m, int axis) {
+  const AxisData& A = m.ax[axis];
+  const size_t nt = (size_t)m.nt;
+  return (A.rec32 ? sizeof(TetRec32) * nt : 0) + (A.rot32 ? 4 * sizeof(TetRot32) * nt : 0) +
+         (A.rec64 ? sizeof(TetRec64) * nt : 0);
+}
+
+size_t mesh_missing_record_bytes(const Mesh& m, int axis, int precision) {
+  const AxisData& A = m.ax[axis];
+  const size_t nt = (size_t)m.nt;
+  size_t b = 0;
+  if (precision == DTFE_MIXED && !A.rec32)
+    b += sizeof(TetRec32) * nt + (m.nt < (1 << 29) ? 4 * sizeof(TetRot32) * nt : 0);
+  // the mixed walk reads FP64 records only when the coordinates are not floats
+  const bool want64 = precision == DTFE_FP64 ||
+                      (!m.fp32_exact && !(m.flags & DTFE_MESH_NO_FP64_REC));
+  if (want64 && !A.rec64) b += sizeof(TetRec64) * nt;
+  return b;
 }
 
 // Frees one axis' walk records (the caller has no map of that axis in flight).

@@ -85,6 +85,10 @@ dtfe_status_t mesh_density(Mesh* m);
 dtfe_status_t mesh_gradients(Mesh* m);
 dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32);
 void mesh_drop_records(Mesh* m, int axis);
+// device bytes of one axis' walk records: held now, and still to build for a
+// map of the given precision
+size_t mesh_record_bytes(const Mesh& m, int axis);
+size_t mesh_missing_record_bytes(const Mesh& m, int axis, int precision);
 // host_mask (optional) replaces the forward-face test with a caller's bitmap
 // (one 32-bit word per tet, faces in bits 0..3)
 dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count_out);

@@ -39,7 +39,6 @@ namespace {
 
 constexpr int kSlots = 3;     // iteration job-table buffers
 constexpr int kInFlight = 2;  // iterations on the GPU at once
-constexpr size_t kRec32Bytes = sizeof(TetRec32), kRec64Bytes = sizeof(TetRec64);
 
 struct Request {
   uint64_t id = 0;
@@ -118,19 +117,10 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 // record bytes a request of (axis, precision) still needs on its mesh
 size_t missing_record_bytes(const Mesh& m, int axis, int precision) {
-  const AxisData& A = m.ax[axis];
-  size_t b = 0;
-  if (precision == DTFE_MIXED && !A.rec32) b += kRec32Bytes * (size_t)m.nt;
-  const bool want64 = precision == DTFE_FP64 ||
-                      (!m.fp32_exact && !(m.flags & DTFE_MESH_NO_FP64_REC));
-  if (want64 && !A.rec64) b += kRec64Bytes * (size_t)m.nt;
-  return b;
+  return mesh_missing_record_bytes(m, axis, precision);
 }
 
-size_t record_bytes(const Mesh& m, int axis) {
-  const AxisData& A = m.ax[axis];
-  return (A.rec32 ? kRec32Bytes * (size_t)m.nt : 0) + (A.rec64 ? kRec64Bytes * (size_t)m.nt : 0);
-}
+size_t record_bytes(const Mesh& m, int axis) { return mesh_record_bytes(m, axis); }
 
 void note_use(Server* S) {
   if (S->in_use > S->peak) S->peak = S->in_use;
@@ -264,7 +254,18 @@ bool admit(Server* S) {
     }
     S->pending.pop_front();
     S->active.push_back(r);
-    const dtfe_status_t s = admit_one(S, r);
+    dtfe_status_t s = admit_one(S, r);
+    if (s == DTFE_ERR_NOMEM) {
+      // the device had less room than the budget assumed: return the pool's
+      // cached map memory, drop every idle (mesh, axis) record set and try
+      // once more
+      release(S, r);
+      cudaStreamSynchronize(S->copy);
+      cudaMemPoolTrimTo(S->pool, 0);
+      make_room(S, S->cfg.device_budget + 1, key);
+      S->active.push_back(r);
+      s = admit_one(S, r);
+    }
     if (s != DTFE_OK) {
       release(S, r);
       fail_request(S, r, s);

@@ -345,14 +345,14 @@ __device__ __forceinline__ double chord32(const TetRec32* __restrict__ R, const 
   return inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
 }
 
-// Fast-step table: for entry face F and the sign bits of the rotated products
-// (e01, e12, e20, a0, a1, a2 = u(0,1), u(1,2), u(2,0), u(3,0), u(3,1), u(3,2)),
-// the rotated slot k (0..2) whose opposite face the ray leaves through, with
-// bit 2 set, when the reference's rule (face_lut_entry on the products in the
-// mesh's own edge order) enters through F; 0 otherwise.  A product of a
-// reversed edge is the exact negative (the reference's formula is
-// antisymmetric in its two vertices), so the mesh-order signs follow from the
-// rotated ones.
+// The reference's rule seen from a rotated record: for entry face F and the
+// sign bits of the rotated products (e01, e12, e20, a0, a1, a2 = u(0,1),
+// u(1,2), u(2,0), u(3,0), u(3,1), u(3,2)), the rotated slot k (0..2) whose
+// opposite face the ray leaves through, with bit 2 set, when the reference's
+// rule (face_lut_entry on the products in the mesh's own edge order) enters
+// through F; 0 otherwise.  A product of a reversed edge is the exact negative
+// (the reference's formula is antisymmetric in its two vertices), so the
+// mesh-order signs follow from the rotated ones.
 __host__ __device__ constexpr unsigned rot_lut_entry(int F, unsigned neg_rot) {
   // rotated pair (p, q) -> product index j and reversal
   unsigned neg = 0;
@@ -379,6 +379,24 @@ __host__ __device__ constexpr unsigned rot_lut_entry(int F, unsigned neg_rot) {
   return (unsigned)rot_inv(F, leave) | 4u;
 }
 
+// The same rule in closed form, the same for every F (the four rotations
+// list their faces with one orientation): the three entry-face products are
+// negative, and the ray leaves through the face opposite the slot k with
+// a(k+1) < 0 and a(k+2) > 0.
+__host__ __device__ constexpr unsigned rot_exit_rule(unsigned neg_rot) {
+  if ((neg_rot & 7u) != 7u) return 0u;
+  const bool n0 = (neg_rot >> 3) & 1u, n1 = (neg_rot >> 4) & 1u, n2 = (neg_rot >> 5) & 1u;
+  return (n1 && !n2) ? 4u : ((n2 && !n0) ? 5u : ((n0 && !n1) ? 6u : 0u));
+}
+
+constexpr bool exit_rule_is_the_reference_rule() {
+  for (int F = 0; F < 4; ++F)
+    for (unsigned v = 0; v < 64; ++v)
+      if (rot_lut_entry(F, v) != rot_exit_rule(v)) return false;
+  return true;
+}
+static_assert(exit_rule_is_the_reference_rule(), "fast-step exit rule differs from the reference's");
+
 template <class T>
 __device__ __forceinline__ T sel3(int k, T a, T b, T c) {
   return k == 0 ? a : (k == 1 ? b : c);
@@ -403,8 +421,8 @@ struct FastStep {
 // such a crossing is not shared with a neighbouring chord, so its error does
 // not cancel.  The general step computes those crossings exactly.
 __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, int ri,
-                                          const unsigned char* __restrict__ lut4, double z_in,
-                                          float f_in, float e_in, double sum, FastStep* o) {
+                                          double z_in, float f_in, float e_in, double sum,
+                                          FastStep* o) {
   const TetRot32* p = C.rot + ri;
   const float4 a = __ldg(&p->xy01), b = __ldg(&p->xy23), z = __ldg(&p->z), f = __ldg(&p->fld);
   const int4 nb = __ldg(&p->nb);
@@ -412,9 +430,10 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   const float x1 = __fsub_rn(__fsub_rn(a.z, r.oxh), r.oxl), y1 = __fsub_rn(__fsub_rn(a.w, r.oyh), r.oyl);
   const float x2 = __fsub_rn(__fsub_rn(b.x, r.oxh), r.oxl), y2 = __fsub_rn(__fsub_rn(b.y, r.oyh), r.oyl);
   const float x3 = __fsub_rn(__fsub_rn(b.z, r.oxh), r.oxl), y3 = __fsub_rn(__fsub_rn(b.w, r.oyh), r.oyl);
-  const float dmax = fmaxf(fmaxf(fmaxf(fabsf(x0), fabsf(y0)), fmaxf(fabsf(x1), fabsf(y1))),
-                           fmaxf(fmaxf(fabsf(x2), fabsf(y2)), fmaxf(fabsf(x3), fabsf(y3))));
-  // the bound of tet_test: FP32 and reference rounding plus the threshold
+  // The line crossed the entry face (the previous step decided its signs), so
+  // the origin lies in the tet's projection and no |relative coordinate|
+  // exceeds the record's extent: the bound of tet_test with that for dmax.
+  const float dmax = __int_as_float(nb.w);
   const float bound = __fmaf_ru(kProdErr * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
   const float e01 = __fmaf_rn(x0, y1, -__fmul_rn(y0, x1));
   const float e12 = __fmaf_rn(x1, y2, -__fmul_rn(y1, x2));
@@ -424,13 +443,15 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   const float a2 = __fmaf_rn(x3, y2, -__fmul_rn(y3, x2));
   const float umin = fminf(fminf(fminf(fabsf(e01), fabsf(e12)), fminf(fabsf(e20), fabsf(a0))),
                            fminf(fabsf(a1), fabsf(a2)));
-  if (!(umin > bound)) return false;
-  const unsigned neg = (__float_as_uint(e01) >> 31) | ((__float_as_uint(e12) >> 31) << 1) |
-                       ((__float_as_uint(e20) >> 31) << 2) | ((__float_as_uint(a0) >> 31) << 3) |
-                       ((__float_as_uint(a1) >> 31) << 4) | ((__float_as_uint(a2) >> 31) << 5);
-  const unsigned code = lut4[((unsigned)(ri & 3) << 6) | neg];
-  if (!(code & 4u)) return false;
-  const int k = (int)(code & 3u);
+  // every sign certain, and the reference's rule (rot_exit_rule) enters here;
+  // sign-bit arithmetic, so that the only branch is the decline
+  const unsigned n0 = __float_as_uint(a0) >> 31, n1 = __float_as_uint(a1) >> 31,
+                 n2 = __float_as_uint(a2) >> 31;
+  const unsigned k0 = n1 & ~n2, k1 = n2 & ~n0, k2 = n0 & ~n1;
+  const unsigned ok = (__float_as_uint(e01) & __float_as_uint(e12) & __float_as_uint(e20)) >> 31 &
+                      (k0 | k1 | k2) & (umin > bound ? 1u : 0u);
+  if (!ok) return false;
+  const int k = (int)(k1 | (k2 << 1));
   const int next = sel3(k, nb.x, nb.y, nb.z);
   if (next < -1) return false;  // a neighbour that does not list this tet
   // exit face: apex (slot 3) and slots i = k+1, j = k+2 (mod 3); the weight of
@@ -623,7 +644,7 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
     }
     if (ri >= 0) {
       FastStep o;
-      if (fast_step(C, r, ri, lut + 64, z_in, f_in, e_in, sum, &o)) {
+      if (fast_step(C, r, ri, z_in, f_in, e_in, sum, &o)) {
         if (visits != nullptr && crossed < max_record) visits[crossed] = cur;
         ++crossed;
         sum += o.contrib;
@@ -674,13 +695,11 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
   return status;
 }
 
-// Shared-memory tables of the walk: the face rule on 64 sign patterns, then
-// the fast-step table (256 entries).
-constexpr int kLutBytes = 64 + 256;
+// Shared-memory table of the general step: the face rule on 64 sign patterns.
+constexpr int kLutBytes = 64;
 
 __device__ __forceinline__ void fill_lut(unsigned char* lut) {
-  for (int i = threadIdx.x; i < kLutBytes; i += blockDim.x)
-    lut[i] = (unsigned char)(i < 64 ? face_lut_entry(i) : rot_lut_entry((i - 64) >> 6, (i - 64) & 63u));
+  for (int i = threadIdx.x; i < kLutBytes; i += blockDim.x) lut[i] = (unsigned char)face_lut_entry(i);
 }
 
 struct MapArgs32 {
@@ -916,15 +935,15 @@ struct Variant32 {
 const Variant32 kVariants32[] = {
     {k_map32<256, 2>, 256, 2, 0}, {k_map32<256, 3>, 256, 3, 0}, {k_map32<256, 4>, 256, 4, 0},
     {k_map32<128, 4>, 128, 4, 0}, {k_map32<128, 6>, 128, 6, 0}, {k_map32<256, 2>, 256, 2, 1},
-    {k_map32<256, 3>, 256, 3, 1},
+    {k_map32<256, 3>, 256, 3, 1}, {k_map32<128, 8>, 128, 8, 0}, {k_map32<64, 16>, 64, 16, 0},
 };
 constexpr int kNumVariants32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
-constexpr int kDefaultVariant32 = 1;  // (256, 3): the usual winner on B200
+constexpr int kDefaultVariant32 = 7;  // (128, 8): the usual winner on B200
 
 typedef void (*BatchKernel32)(const BatchJob32*, int, long long, unsigned long long*);
 const BatchKernel32 kBatch32[] = {k_batch32<256, 2>, k_batch32<256, 3>, k_batch32<256, 4>,
                                   k_batch32<128, 4>, k_batch32<128, 6>, k_batch32<256, 2>,
-                                  k_batch32<256, 3>};
+                                  k_batch32<256, 3>, k_batch32<128, 8>, k_batch32<64, 16>};
 static_assert(sizeof(kBatch32) / sizeof(kBatch32[0]) == kNumVariants32, "one batch kernel per variant");
 
 // Checks that an axis has what the mixed walk reads.

@@ -29,7 +29,10 @@ struct __align__(16) TetRot32 {
   float4 fld;   // (rho0, rho1, rho2, rho3)
   int4 nb;      // x..z: record 4*n + F' of the neighbour n across the face opposite
                 // slot 0..2, F' the face of n shared with this tet; -1 on the hull,
-                // INT_MIN when n does not list this tet; w: the tet id
+                // INT_MIN when n does not list this tet; w: the float bits of the
+                // extent of the tet's projection (largest x or y difference of
+                // two vertices, rounded up), a bound on |vertex - origin| for
+                // any ray that crossed one of its faces
 };
 static_assert(sizeof(TetRot32) == 80, "TetRot32 layout");
 
