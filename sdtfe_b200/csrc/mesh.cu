@@ -216,6 +216,21 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
         hi[c] = fmaxf(hi[c], (float)q[s][c]);
       }
     const float ext = __fmul_ru(fmaxf(__fsub_ru(hi[0], lo[0]), __fsub_ru(hi[1], lo[1])), 1.0000010f);
+    // Condition of the FP32 field value rho3 + grad . (p - v3) at a point p
+    // of the tet: the magnitudes summed over the least vertex value, a bound
+    // on the field there (a convex combination of the vertex values).  Its
+    // rounding is a few units of roundoff times this; above kFieldCond the
+    // walk evaluates the tet in FP64 (slivers, whose gradient terms cancel,
+    // and vertex values of mixed sign or zero).
+    double rmin = fabs(p[0].w), rmax = rmin;
+#pragma unroll
+    for (int s = 1; s < 4; ++s) {
+      rmin = fmin(rmin, fabs(p[s].w));
+      rmax = fmax(rmax, fabs(p[s].w));
+    }
+    const double cond = (rmax + (fabs(g[0]) + fabs(g[1])) * (double)ext +
+                         fabs(g[2]) * (double)(zmax - zmin)) / rmin;
+    const int fp64_field = (cond <= kFieldCond) ? 0 : (int)0x80000000u;  // also NaN, rmin = 0
 #pragma unroll
     for (int F = 0; F < 4; ++F) {
       const int s0 = rot_slot(F, 0), s1 = rot_slot(F, 1), s2 = rot_slot(F, 2), s3 = rot_slot(F, 3);
@@ -223,8 +238,8 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
       r.xy01 = make_float4((float)q[s0][0], (float)q[s0][1], (float)q[s1][0], (float)q[s1][1]);
       r.xy23 = make_float4((float)q[s2][0], (float)q[s2][1], (float)q[s3][0], (float)q[s3][1]);
       r.z = make_float4((float)q[s0][2], (float)q[s1][2], (float)q[s2][2], (float)q[s3][2]);
-      r.fld = make_float4((float)p[s0].w, (float)p[s1].w, (float)p[s2].w, (float)p[s3].w);
-      r.nb = make_int4(nxt[s0], nxt[s1], nxt[s2], __float_as_int(ext));
+      r.fld = make_float4((float)p[s3].w, (float)g[0], (float)g[1], (float)g[2]);
+      r.nb = make_int4(nxt[s0], nxt[s1], nxt[s2], __float_as_int(ext) | fp64_field);
       rot[4 * (size_t)t + F] = r;
     }
   }

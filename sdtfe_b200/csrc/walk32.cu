@@ -7,29 +7,40 @@
 // taken relative to the ray origin (the origin split into a float hi/lo
 // pair) together with a bound on its FP32 error.  When every product clears
 // the reference's threshold by more than that bound plus the reference's own
-// FP64 rounding, all six reference signs are known and nonzero, and a 64-entry
-// table maps them to the reference's enter/leave choice.  Otherwise the tet
-// is re-tested with the reference's FP64 products and operands and the
-// general face rule (zero signs, perturbation) applies, exactly as in the FP64
-// walk.  Every ray therefore visits the FP64 path's tets in the FP64 path's
-// order.
+// FP64 rounding, all six reference signs are known and nonzero, and the
+// reference's enter/leave rule follows from them.  Otherwise the tet is
+// re-tested with the reference's FP64 products and operands and the general
+// face rule (zero signs, perturbation) applies, exactly as in the FP64 walk.
+// Every ray therefore visits the FP64 path's tets in the FP64 path's order.
 //
-// What is FP32.  The integral.  Only the exit crossing of each tet is
-// computed: its position is vertex A's z plus a barycentric offset (weights =
-// the exit face's signed edge terms over their sum; the terms share one sign,
-// so there is no cancellation) and its field value is the same barycentric
-// mix of the face's vertex densities.  Both are carried into the next tet as
-// its entry crossing, so consecutive chords share their interface exactly and
-// the chord lengths telescope: an ill-conditioned face (nearly parallel to
-// the ray) only moves an interface, which the continuity of the linear field
-// makes a second-order effect.  The chord contributes (f_in + f_out)/2 times
-// its length - exact for the linear field, and the reference's value
-// (rho_A + grad.(p_mid - v_A)) * dz (src/dtfe.c:356-369) in exact arithmetic.
-// Crossing positions and the ray's sum are FP64 (a float vertex z plus a float
-// offset, added exactly; one multiply-add per chord).  The midpoint-in-slab
-// test uses a guard band; inside it the reference's FP64 midpoint decides.  A tet whose entry face is not the face it was reached
-// through (turn-arounds, perturbations) computes its own entry crossing, as
-// the reference does.
+// Two kinds of step.  A tet entered through a face shared with the previous
+// tet takes the fast step on its record for that entry face (TetRot32): the
+// entry face's vertices sit in fixed slots, so the six products, the exit
+// face (closed form, proven equal to the reference's rule by static_assert),
+// the exit crossing and the chord need no table and no data-dependent
+// indexing beyond picking one of three exit faces.  Anything the fast step
+// cannot decide exactly - an uncertain sign, a rule that does not enter
+// through the known face, an ill-conditioned or hull crossing whose error
+// would matter, a midpoint in the slab's guard band, a tet whose FP32 field
+// value is not trusted - goes to the general step (mesh-order record, FP64
+// where needed), which also takes the first tet of every ray.
+//
+// What is FP32.  The crossings and the field value.  The exit crossing's z is
+// the apex z plus a barycentric offset (weights = the exit face's signed edge
+// products over their sum; same sign, no cancellation), carried into the next
+// tet as its entry, so consecutive chords share their interface exactly and
+// the chord lengths telescope.  The chord's value is the reference's own
+// formula (src/dtfe.c:363-368): the tet's linear field rho + grad.(p - v) at
+// the point p of the ray line at the chord's midpoint, here from the apex.
+// p is on the line, so an error in a crossing only moves a chord end shared
+// with the neighbour, which the continuity of the linear field makes a
+// second-order effect.  Tets whose FP32 field value could cancel badly
+// (magnitudes over least vertex value above kFieldCond: slivers, extreme
+// density contrast) are evaluated from the mesh's FP64 vertex, density and
+// gradient in the general step.  Crossing positions and the ray's sum are
+// FP64 (a float vertex z plus a float offset, added exactly).  The midpoint-
+// in-slab test uses each crossing's error bound; inside that band the
+// reference's FP64 midpoint decides.
 //
 // Compiled with -fmad=false like walk.cu: the sample positions and the point
 // location it shares with the FP64 walk must round as the reference does;
@@ -68,6 +79,9 @@ struct MixConf {
   int exact32;                         // the float coordinates are the doubles
   const TetRot32* __restrict__ rot;    // records per entry face (NULL: general steps only)
   const TetRec32* __restrict__ rec32;  // the mesh-order records
+  const double4* __restrict__ pos;     // vertices and their densities, original frame
+  const double* __restrict__ grad;     // per-tet gradients, original frame
+  int axis;                            // projection axis (frame permutation)
   // Chord midpoints inside (zlo_in, zhi_in) are surely inside the slab for
   // every tet of the mesh; others are tested against their own error bound.
   double zlo_in, zhi_in;
@@ -320,18 +334,32 @@ __device__ __noinline__ double midpoint64(const TetRec32* __restrict__ R32,
   return d / 2 + zi;
 }
 
-// One chord's contribution: (f_in + f_out)/2 times its length when its
-// midpoint lies in the slab (src/dtfe.c:356-369).  Crossing positions are
+// The reference's chord value (src/dtfe.c:363-368) in FP64: the tet's linear
+// field rho_A + grad . (p - A) at the point of the ray line at height zmid,
+// from the mesh's FP64 vertex, density and gradient.
+__device__ __noinline__ double field64(const MixConf& C, int t, double ox, double oy, double zmid) {
+  const int4 v = __ldg(&C.rec32[t].aux);
+  const double4 A = C.pos[v.x];
+  double ax, ay, az, gx, gy, gz;
+  permute3(C.axis, A.x, A.y, A.z, &ax, &ay, &az);
+  permute3(C.axis, C.grad[3 * (size_t)t], C.grad[3 * (size_t)t + 1], C.grad[3 * (size_t)t + 2], &gx,
+           &gy, &gz);
+  return A.w + gx * (ox - ax) + gy * (oy - ay) + gz * (zmid - az);
+}
+
+// One chord's contribution: the field at its midpoint on the ray line times
+// its length, when the midpoint lies in the slab (src/dtfe.c:356-369).  Crossing positions are
 // doubles (a float vertex z plus a float offset, summed exactly), so the exit
 // of one chord is bit-for-bit the entry of the next and the chord lengths
 // telescope.  The slab test compares the float midpoint with a guard band;
 // inside the band the reference's FP64 midpoint decides.
 __device__ __forceinline__ double chord32(const TetRec32* __restrict__ R, const MixConf& C,
                                           const RayState& r, int t, int enter, int leave,
-                                          double z_in, float f_in, double z_out, float f_out,
-                                          float hz, float e_inout, int* fallbacks) {
+                                          double z_in, double z_out, float hz, float e_inout,
+                                          int* fallbacks) {
   const double d = z_out - z_in;
-  const float zm = (float)(z_in + 0.5 * d);
+  const double zmid = z_in + 0.5 * d;
+  const float zm = (float)zmid;
   // float rounding of the midpoint plus the crossings' own error bounds
   const float guard = 64.f * kEps * (fabsf(zm) + hz) + e_inout;
   bool inside;
@@ -342,7 +370,9 @@ __device__ __forceinline__ double chord32(const TetRec32* __restrict__ R, const 
     inside = zmd > C.z0d && zmd < C.z1d;
     ++*fallbacks;
   }
-  return inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
+  if (!inside) return 0.0;
+  ++*fallbacks;
+  return field64(C, t, r.ox, r.oy, zmid) * d;
 }
 
 // The reference's rule seen from a rotated record: for entry face F and the
@@ -405,7 +435,6 @@ __device__ __forceinline__ T sel3(int k, T a, T b, T c) {
 struct FastStep {
   double z_out;    // exit crossing
   double contrib;  // the chord's share of the integral
-  float f_out;     // field at the exit crossing
   float e_out;     // bound on the exit crossing's z error
   int next;        // record of the next tet; -1: the ray left the mesh here
 };
@@ -421,8 +450,7 @@ struct FastStep {
 // such a crossing is not shared with a neighbouring chord, so its error does
 // not cancel.  The general step computes those crossings exactly.
 __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, int ri,
-                                          double z_in, float f_in, float e_in, double sum,
-                                          FastStep* o) {
+                                          double z_in, float e_in, double sum, FastStep* o) {
   const TetRot32* p = C.rot + ri;
   const float4 a = __ldg(&p->xy01), b = __ldg(&p->xy23), z = __ldg(&p->z), f = __ldg(&p->fld);
   const int4 nb = __ldg(&p->nb);
@@ -433,7 +461,7 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   // The line crossed the entry face (the previous step decided its signs), so
   // the origin lies in the tet's projection and no |relative coordinate|
   // exceeds the record's extent: the bound of tet_test with that for dmax.
-  const float dmax = __int_as_float(nb.w);
+  const float dmax = __int_as_float(nb.w & 0x7fffffff);
   const float bound = __fmaf_ru(kProdErr * kEps * dmax, dmax, __fmaf_ru(r.e_coef, dmax, r.thr_hi));
   const float e01 = __fmaf_rn(x0, y1, -__fmul_rn(y0, x1));
   const float e12 = __fmaf_rn(x1, y2, -__fmul_rn(y1, x2));
@@ -448,7 +476,9 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   const unsigned n0 = __float_as_uint(a0) >> 31, n1 = __float_as_uint(a1) >> 31,
                  n2 = __float_as_uint(a2) >> 31;
   const unsigned k0 = n1 & ~n2, k1 = n2 & ~n0, k2 = n0 & ~n1;
-  const unsigned ok = (__float_as_uint(e01) & __float_as_uint(e12) & __float_as_uint(e20)) >> 31 &
+  // (sign bit of nb.w: the tet's FP32 field value is not trusted)
+  const unsigned ok = (__float_as_uint(e01) & __float_as_uint(e12) & __float_as_uint(e20) &
+                       ~(unsigned)nb.w) >> 31 &
                       (k0 | k1 | k2) & (umin > bound ? 1u : 0u);
   if (!ok) return false;
   const int k = (int)(k1 | (k2 << 1));
@@ -460,14 +490,12 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   const float wi = -sel3(k, a2, a0, a1);
   const float wj = sel3(k, a1, a2, a0);
   const float zi = sel3(k, z.y, z.z, z.x), zj = sel3(k, z.z, z.x, z.y);
-  const float fi = sel3(k, f.y, f.z, f.x), fj = sel3(k, f.z, f.x, f.y);
   const float den = w3 + wi + wj;
   const float rr = __fdividef(1.f, den);
   const float cond = 3.f * bound * fabsf(rr);  // relative error of the weights
   const float hi = zi - z.w, hj = zj - z.w;
   if (!(cond <= kCrossingTol)) return false;  // ill-conditioned
   const float dzr = rr * __fmaf_rn(wj, hj, wi * hi);
-  const float f_out = rr * __fmaf_rn(wj, fj, __fmaf_rn(wi, fi, w3 * f.w));
   // z error: the weights' error over the face's height above the apex, plus
   // the rounding of the offset (the double sum with the apex z is exact)
   const float e_out = (cond + 8.f * kEps) * fmaxf(fabsf(hi), fabsf(hj));
@@ -481,16 +509,19 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
     if (!(fabsf(d0) > g && fabsf(d1) > g)) return false;  // the reference's midpoint decides
     inside = d0 > 0.f && d1 < 0.f;
   }
-  const double contrib = inside ? (double)(0.5f * (f_in + f_out)) * d : 0.0;
+  // the reference's chord value (src/dtfe.c:363-368) from the apex: the
+  // tet's linear field rho3 + grad . (p - v3) at the point p of the ray line
+  // at the chord's midpoint.  p lies on the line, so errors of the crossings
+  // only move chord ends, shared with the neighbours: they cancel to first
+  // order.  fld = (rho3, grad_x, grad_y, grad_z); (x3, y3) = v3 - origin.
+  const float zr = (float)(zm - (double)z.w);
+  const float g = __fmaf_rn(f.w, zr, __fmaf_rn(-f.z, y3, __fmaf_rn(-f.y, x3, f.x)));
+  const double contrib = inside ? (double)g * d : 0.0;
   if (next == -1 && inside) {
-    // what the FP32 exit can add: its field error (the weights' error over
-    // the face's largest vertex value) over half the chord, and its z error
-    const float e_f = (cond + 8.f * kEps) * fmaxf(fmaxf(fabsf(fi), fabsf(fj)), fabsf(f.w));
-    const float e_c = 0.5f * (e_f * fabsf((float)d) + fabsf(f_in + f_out) * e_out);
-    if (!(e_c <= 1e-7f * (float)fabs(sum + contrib))) return false;
+    // the exit crossing's z error times the field is not cancelled
+    if (!(fabsf(g) * e_out <= 1e-7f * (float)fabs(sum + contrib))) return false;
   }
   o->z_out = z_out;
-  o->f_out = f_out;
   o->e_out = e_out;
   o->contrib = contrib;
   o->next = next;
@@ -510,10 +541,10 @@ __device__ __forceinline__ int rot_next(const MixConf& C, int t, int m) {
 struct WalkState {
   RayState r;
   double sum, z_in;
-  float f_in, e_in;  // e_in: bound on z_in's error
+  float e_in;        // bound on z_in's error
   uint64_t ctr;      // perturbation draws so far
   int crossed, fallbacks, cur, prev, ri;
-  bool carried;      // z_in / f_in hold the crossing of the face shared with prev
+  bool carried;      // z_in holds the crossing of the face shared with prev
 };
 
 constexpr int kWalkOn = -1;  // general_step: the walk continues
@@ -568,28 +599,25 @@ __device__ __noinline__ int general_step(const TetRec32* __restrict__ R, const M
   if (!w.carried || nb_at(nb, enter) != w.prev) {
     const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, enter, r.ox, r.oy);
     w.z_in = c.x;
-    w.f_in = (float)c.y;
     w.e_in = 0.f;
     ++w.fallbacks;
   }
   // exit crossing: FP32 unless it leaves the mesh (not shared with a
   // neighbouring chord) or is ill-conditioned
-  float dzo, f_out, e_out = 0.f;
+  float dzo, f_unused, e_out = 0.f;
   double z_out;
-  const float cond = crossing(leave, u, bmax, v, &dzo, &f_out);
+  const float cond = crossing(leave, u, bmax, v, &dzo, &f_unused);
   const float hz = fmaxf(fmaxf(fabsf(v.z[1] - v.z[0]), fabsf(v.z[2] - v.z[0])),
                          fabsf(v.z[3] - v.z[0]));
   if (nb_at(nb, leave) == -1 || !(cond <= kCrossingTol)) {
     const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
     z_out = c.x;
-    f_out = (float)c.y;
     ++w.fallbacks;
   } else {
     z_out = (double)v.z[0] + (double)dzo;
     e_out = (cond + 8.f * kEps) * hz;
   }
-  w.sum += chord32(R, C, r, cur, enter, leave, w.z_in, w.f_in, z_out, f_out, hz, w.e_in + e_out,
-                   &w.fallbacks);
+  w.sum += chord32(R, C, r, cur, enter, leave, w.z_in, z_out, hz, w.e_in + e_out, &w.fallbacks);
 
   // move on (src/dtfe.c:300-309)
   int m = leave;
@@ -601,7 +629,6 @@ __device__ __noinline__ int general_step(const TetRec32* __restrict__ R, const M
   if (nx == -1) return kRayOk;
   if (m == leave) {
     w.z_in = z_out;
-    w.f_in = f_out;
     w.e_in = e_out;
   }  // else the enter face's crossing, already in z_in
   w.carried = true;
@@ -631,7 +658,7 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
   ray_setup(r, C);
   uint64_t ctr = 0;
   double sum = 0.0, z_in = 0.0;
-  float f_in = 0.f, e_in = 0.f;
+  float e_in = 0.f;
   bool carried = false;
   int crossed = 0, fallbacks = 0;
   int cur = ft, prev = -1;
@@ -644,7 +671,7 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
     }
     if (ri >= 0) {
       FastStep o;
-      if (fast_step(C, r, ri, z_in, f_in, e_in, sum, &o)) {
+      if (fast_step(C, r, ri, z_in, e_in, sum, &o)) {
         if (visits != nullptr && crossed < max_record) visits[crossed] = cur;
         ++crossed;
         sum += o.contrib;
@@ -653,7 +680,6 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
           break;
         }
         z_in = o.z_out;
-        f_in = o.f_out;
         e_in = o.e_out;
         prev = cur;
         ri = o.next;
@@ -665,7 +691,6 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
     w.r = r;
     w.sum = sum;
     w.z_in = z_in;
-    w.f_in = f_in;
     w.e_in = e_in;
     w.ctr = ctr;
     w.crossed = crossed;
@@ -678,7 +703,6 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
     r = w.r;
     sum = w.sum;
     z_in = w.z_in;
-    f_in = w.f_in;
     e_in = w.e_in;
     ctr = w.ctr;
     crossed = w.crossed;
@@ -897,6 +921,9 @@ MixConf mix_conf(const Mesh& m, int axis, double z0, double lz, double dist, uin
   C.exact32 = m.fp32_exact ? 1 : 0;
   C.rot = m.ax[axis].rot32;
   C.rec32 = m.ax[axis].rec32;
+  C.pos = m.pos;
+  C.grad = m.grad;
+  C.axis = axis;
   // A midpoint from FP32-derived crossings is within tol * H of the
   // reference's (each crossing within tol times its tet's height, H the
   // largest) plus float rounding of positions of magnitude up to Z.

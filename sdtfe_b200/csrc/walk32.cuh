@@ -26,14 +26,19 @@ struct __align__(16) TetRot32 {
   float4 xy01;  // (x0, y0, x1, y1)
   float4 xy23;  // (x2, y2, x3, y3)
   float4 z;     // (z0, z1, z2, z3)
-  float4 fld;   // (rho0, rho1, rho2, rho3)
+  float4 fld;   // (rho3, grad_x, grad_y, grad_z): the tet's linear field from the
+                // apex, gradient in the projected frame
   int4 nb;      // x..z: record 4*n + F' of the neighbour n across the face opposite
                 // slot 0..2, F' the face of n shared with this tet; -1 on the hull,
                 // INT_MIN when n does not list this tet; w: the float bits of the
                 // extent of the tet's projection (largest x or y difference of
                 // two vertices, rounded up), a bound on |vertex - origin| for
-                // any ray that crossed one of its faces
+                // any ray that crossed one of its faces, with the sign bit set
+                // when the FP32 field value is not trusted (kFieldCond)
 };
+// largest field condition (magnitudes over least vertex value) the FP32
+// field value is used for
+constexpr double kFieldCond = 4096.0;
 static_assert(sizeof(TetRot32) == 80, "TetRot32 layout");
 
 // Original vertex slot of rotated slot k for entry face F, and its inverse;
