@@ -278,7 +278,8 @@ __global__ void k_hull_mask(const double4* __restrict__ pos, const int4* __restr
 // a6 part 1: emit hull triangles in (tet, face) order with the reference's
 // corner order per face (src/triangulate.c:325-355).
 __global__ void k_hull_emit(const int4* __restrict__ rows, int nt, const uint32_t* __restrict__ mask,
-                            const int* __restrict__ off, int* __restrict__ tri_rows) {
+                            const int* __restrict__ off, int* __restrict__ tri_rows,
+                            signed char* __restrict__ tri_face) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   const uint32_t m = mask[t] & 0xFu;
@@ -290,6 +291,7 @@ __global__ void k_hull_emit(const int4* __restrict__ rows, int nt, const uint32_
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     if (!(m & (1u << f))) continue;
+    tri_face[k] = (signed char)f;
     int* r = tri_rows + 8 * (size_t)k++;
     r[0] = vid[ta[f]];
     r[1] = vid[tb[f]];
@@ -632,11 +634,17 @@ dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count
     m->bytes -= sizeof(int) * 8 * (size_t)(A.n_tri ? A.n_tri : 1);
     A.tri_rows = nullptr;
   }
+  if (A.tri_face) {
+    cudaFree(A.tri_face);
+    m->bytes -= (size_t)(A.n_tri ? A.n_tri : 1);
+    A.tri_face = nullptr;
+  }
   SDTFE_TRY(dmalloc(&A.tri, n_tri, m));
   SDTFE_TRY(dmalloc(&A.tri_rows, 8 * (size_t)n_tri, m));
+  SDTFE_TRY(dmalloc(&A.tri_face, n_tri, m));
   A.n_tri = n_tri;
   if (nt) {
-    k_hull_emit<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, mask, off, A.tri_rows);
+    k_hull_emit<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, mask, off, A.tri_rows, A.tri_face);
     count_launch();
   }
   // vertex -> hull triangle lists for the edge matching
@@ -682,6 +690,7 @@ void mesh_free(Mesh* m) {
     dfree(A.rot32, 4 * (size_t)m->nt, m);
     dfree(A.tri, A.n_tri, m);
     dfree(A.tri_rows, 8 * (size_t)A.n_tri, m);
+    dfree(A.tri_face, A.n_tri, m);
   }
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);

@@ -51,6 +51,7 @@ struct AxisData {
   int n_tri = 0;
   TriRec64* tri = nullptr;  // device, n_tri records
   int* tri_rows = nullptr;  // device, n_tri * 8 ints in the reference's tri_data layout
+  signed char* tri_face = nullptr;  // device, n_tri: the tet face (0..3) under each triangle
   // walk records in this axis' projected frame (built on demand, per precision)
   TetRec64* rec64 = nullptr;
   TetRec32* rec32 = nullptr;

@@ -117,41 +117,49 @@ __global__ void __launch_bounds__(256) k_map64(const MapArgs64 a) {
   map_tile64(a, blockIdx.x, s_val, s_ok);
 }
 
-// Persistent batch over several maps (see k_batch32 in walk32.cu).
+// Persistent batch over several maps (see k_batch32 in walk32.cu): thread 0
+// claims the next tile while the block walks the current one.
+__device__ __forceinline__ void claim_tile64(const BatchJob64* __restrict__ jobs, int n_jobs,
+                                             unsigned long long* __restrict__ queue,
+                                             long long* tile, int* job) {
+  const long long t = (long long)atomicAdd(queue, 1ull);
+  int lo = 0, hi = n_jobs - 1;  // last job whose first tile <= t
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (__ldg(&jobs[mid].first) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  *tile = t;
+  *job = lo;
+}
+
 __global__ void __launch_bounds__(256) k_batch64(const BatchJob64* __restrict__ jobs, int n_jobs,
                                                  long long total_tiles,
                                                  unsigned long long* __restrict__ queue) {
   extern __shared__ double s_val[];
   __shared__ MapArgs64 s_args;
-  __shared__ long long s_tile;
-  __shared__ int s_job;
+  __shared__ long long s_tile[2];
+  __shared__ int s_job[2];
+  if (threadIdx.x == 0) claim_tile64(jobs, n_jobs, queue, &s_tile[0], &s_job[0]);
+  __syncthreads();
   int cur_job = -1;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      s_tile = (long long)atomicAdd(queue, 1ull);
-      int lo = 0, hi = n_jobs - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (jobs[mid].first <= s_tile) lo = mid;
-        else hi = mid - 1;
-      }
-      s_job = lo;
-    }
-    __syncthreads();
-    const long long tile = s_tile;
-    const int j = s_job;
+  for (int it = 0;; ++it) {
+    const int slot = it & 1;
+    const long long tile = s_tile[slot];
+    const int j = s_job[slot];
     if (tile >= total_tiles) break;
-    if (j != cur_job) {
+    if (threadIdx.x == 0) claim_tile64(jobs, n_jobs, queue, &s_tile[slot ^ 1], &s_job[slot ^ 1]);
+    if (j != cur_job) {  // j is the same for the whole block
       const int* src = reinterpret_cast<const int*>(&jobs[j].args);
       int* dst = reinterpret_cast<int*>(&s_args);
       for (int k = threadIdx.x; k < (int)(sizeof(MapArgs64) / sizeof(int)); k += blockDim.x)
         dst[k] = src[k];
       cur_job = j;
+      __syncthreads();
     }
-    __syncthreads();
     unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val + s_args.TW * s_args.TH * s_args.S);
     map_tile64(s_args, jobs[j].tile0 + (int)(tile - jobs[j].first), s_val, s_ok);
-    __syncthreads();
+    __syncthreads();  // s_val, s_args and the claimed slot are reused next
   }
 }
 

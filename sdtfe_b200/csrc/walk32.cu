@@ -78,6 +78,7 @@ struct MixConf {
   const TetRec64* __restrict__ rec64;  // exact coordinates when the floats are not
   int exact32;                         // the float coordinates are the doubles
   const TetRot32* __restrict__ rot;    // records per entry face (NULL: general steps only)
+  const signed char* __restrict__ tri_face;  // the tet face under each hull triangle
   const TetRec32* __restrict__ rec32;  // the mesh-order records
   const double4* __restrict__ pos;     // vertices and their densities, original frame
   const double* __restrict__ grad;     // per-tet gradients, original frame
@@ -640,11 +641,13 @@ __device__ __noinline__ int general_step(const TetRec32* __restrict__ R, const M
 
 // The mixed walk.  Same control flow as walk64 (src/dtfe.c:247-374); returns
 // the status, the integral in *rho and the crossing count.  A tet entered
-// through a face shared with the previous one (the crossing there carried
-// over) takes the fast step on its record for that entry face; the first
-// tet, and any tet the fast step declines, takes the general step.
+// through a known face, with the crossing there in hand, takes the fast step
+// on its record for that entry face; any tet the fast step declines takes the
+// general step.  The first tet is entered through the hull triangle the
+// sample was located in (ft_tri; its face is known from the hull build), at
+// the exact crossing.
 __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixConf& C, int ft,
-                                      double x, double y, uint64_t ray,
+                                      int ft_tri, double x, double y, uint64_t ray,
                                       const unsigned char* __restrict__ lut, double* rho_out,
                                       int* crossed_out, int* fallbacks_out, int* visits,
                                       int max_record) {
@@ -664,6 +667,13 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
   int cur = ft, prev = -1;
   int ri = -1;  // cur's record for its entry face (-1: general step)
   int status = kWalkOn;
+  if (C.rot && ft_tri >= 0) {  // enter through the located hull face, exactly
+    const int F = C.tri_face[ft_tri];
+    z_in = exact_crossing(R, C.rec64, C.exact32, C.lz, ft, F, r.ox, r.oy).x;
+    ++fallbacks;
+    carried = true;
+    ri = 4 * ft + F;
+  }
   for (;;) {
     if (crossed >= C.max_visits) {
       status = kRayBudget;
@@ -698,7 +708,8 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
     w.cur = cur;
     w.prev = prev;
     w.ri = -1;
-    w.carried = carried;
+    // the first tet decides its own entry face (its exact crossing is recomputed)
+    w.carried = carried && crossed > 0;
     status = general_step(R, C, ray, lut, w, visits, max_record);
     r = w.r;
     sum = w.sum;
@@ -791,10 +802,10 @@ __device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
       const double xt = x + sdtfe_sample_u01(a.C.seed, (uint64_t)p, (uint32_t)s, 0) * a.scale;
       const double yt = y + sdtfe_sample_u01(a.C.seed, (uint64_t)p, (uint32_t)s, 1) * a.scale;
       const uint64_t rid = (uint64_t)p * (uint64_t)a.S + (uint64_t)s;
-      int ft = -1;
-      if (a.n_tri > 0) ft = locate64(a.tri, 0, xt, yt, a.loc_budget, &status);
+      int ft = -1, ft_tri = -1;
+      if (a.n_tri > 0) ft = locate64(a.tri, 0, xt, yt, a.loc_budget, &status, &ft_tri);
       if (ft >= 0)
-        status = walk32(a.rec, a.C, ft, xt, yt, rid, lut, &v, &crossed, &fb, nullptr, 0);
+        status = walk32(a.rec, a.C, ft, ft_tri, xt, yt, rid, lut, &v, &crossed, &fb, nullptr, 0);
       if (status != kRayOk) v = 0.0;
       if (a.ray_rho) {
         a.ray_rho[rid] = v;
@@ -838,6 +849,22 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_map32(const __grid_constant__ M
 // counts), so uneven maps share the GPU without a tail per map.  Job j owns
 // global tiles [first[j], first[j+1]) and maps them to its own tiles
 // [tile0, tile0 + count).  The job's arguments are staged in shared memory.
+// Thread 0 claims the next tile (and finds its job) while the block walks the
+// current one, so the claim's latency is hidden.
+__device__ __forceinline__ void claim_tile(const BatchJob32* __restrict__ jobs, int n_jobs,
+                                           unsigned long long* __restrict__ queue,
+                                           long long* tile, int* job) {
+  const long long t = (long long)atomicAdd(queue, 1ull);
+  int lo = 0, hi = n_jobs - 1;  // last job whose first tile <= t
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (__ldg(&jobs[mid].first) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  *tile = t;
+  *job = lo;
+}
+
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_batch32(const BatchJob32* __restrict__ jobs, int n_jobs, long long total_tiles,
@@ -845,36 +872,30 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   extern __shared__ double s_val32[];
   __shared__ unsigned char s_lut[kLutBytes];
   __shared__ MapArgs32 s_args;
-  __shared__ long long s_tile;
-  __shared__ int s_job;
+  __shared__ long long s_tile[2];
+  __shared__ int s_job[2];
   fill_lut(s_lut);
+  if (threadIdx.x == 0) claim_tile(jobs, n_jobs, queue, &s_tile[0], &s_job[0]);
+  __syncthreads();
   int cur_job = -1;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      s_tile = (long long)atomicAdd(queue, 1ull);
-      int lo = 0, hi = n_jobs - 1;  // last job whose first tile <= s_tile
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (jobs[mid].first <= s_tile) lo = mid;
-        else hi = mid - 1;
-      }
-      s_job = lo;
-    }
-    __syncthreads();
-    const long long tile = s_tile;
-    const int j = s_job;
+  for (int it = 0;; ++it) {
+    const int slot = it & 1;
+    const long long tile = s_tile[slot];
+    const int j = s_job[slot];
     if (tile >= total_tiles) break;
-    if (j != cur_job) {  // stage the job's arguments
+    // the next claim goes to the other slot, read only after the end-of-tile barrier
+    if (threadIdx.x == 0) claim_tile(jobs, n_jobs, queue, &s_tile[slot ^ 1], &s_job[slot ^ 1]);
+    if (j != cur_job) {  // stage the job's arguments (j is the same for the whole block)
       const int* src = reinterpret_cast<const int*>(&jobs[j].args);
       int* dst = reinterpret_cast<int*>(&s_args);
       for (int k = threadIdx.x; k < (int)(sizeof(MapArgs32) / sizeof(int)); k += BLOCK)
         dst[k] = src[k];
       cur_job = j;
+      __syncthreads();
     }
-    __syncthreads();
     unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + s_args.TW * s_args.TH * s_args.S);
     map_tile32<BLOCK>(s_args, jobs[j].tile0 + (int)(tile - jobs[j].first), s_lut, s_val32, s_ok);
-    __syncthreads();  // s_val, s_args and s_tile are reused by the next tile
+    __syncthreads();  // s_val, s_args and the claimed slot are reused next
   }
 }
 
@@ -894,9 +915,10 @@ __global__ void __launch_bounds__(128) k_trace32(const TetRec32* __restrict__ re
   if (i >= n_rays) return;
   int st = kRayMiss, c = 0, fb = 0;
   double v = 0.0;
-  const int ft = n_tri > 0 ? locate64(tri, 0, xs[i], ys[i], loc_budget, &st) : -1;
+  int ft_tri = -1;
+  const int ft = n_tri > 0 ? locate64(tri, 0, xs[i], ys[i], loc_budget, &st, &ft_tri) : -1;
   if (ft >= 0)
-    st = walk32(rec, C, ft, xs[i], ys[i], (uint64_t)i, s_lut, &v, &c, &fb,
+    st = walk32(rec, C, ft, ft_tri, xs[i], ys[i], (uint64_t)i, s_lut, &v, &c, &fb,
                 visits ? visits + (size_t)i * max_record : nullptr, max_record);
   rho[i] = st == kRayOk ? v : 0.0;
   crossed[i] = c;
@@ -920,6 +942,7 @@ MixConf mix_conf(const Mesh& m, int axis, double z0, double lz, double dist, uin
   C.rec64 = m.ax[axis].rec64;
   C.exact32 = m.fp32_exact ? 1 : 0;
   C.rot = m.ax[axis].rot32;
+  C.tri_face = m.ax[axis].tri_face;
   C.rec32 = m.ax[axis].rec32;
   C.pos = m.pos;
   C.grad = m.grad;

@@ -147,8 +147,11 @@ __device__ __forceinline__ Hit64 ray_tet64(const Ray64& r, const double2 xy[4], 
 // ---------------------------------------------------------------------------
 // a7: visibility walk on the projected hull, from triangle `start`
 // (src/dtfe.c:518-552).  Returns the tet under the query point or -1.
+// Returns the tet under the hull triangle containing (qx, qy); *tri_out (if
+// given) receives the triangle.
 __device__ __forceinline__ int locate64(const TriRec64* __restrict__ tri, int start, double qx,
-                                        double qy, int max_steps, int* status) {
+                                        double qy, int max_steps, int* status,
+                                        int* tri_out = nullptr) {
   int cur = start;
   int steps = 0;
   *status = kRayOk;
@@ -179,6 +182,7 @@ __device__ __forceinline__ int locate64(const TriRec64* __restrict__ tri, int st
       cur = nb.y;  // across c-a
       continue;
     }
+    if (tri_out) *tri_out = cur;
     return nb.w;
   } while (cur != -1);
   *status = kRayMiss;
