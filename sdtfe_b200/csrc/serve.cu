@@ -616,6 +616,10 @@ dtfe_status_t dtfe_server_submit(dtfe_server_t S, int mesh_id, const dtfe_map_pa
     delete r;
     return set_error(DTFE_ERR_INVALID, "server is shutting down");
   }
+  if (S->fatal != DTFE_OK) {  // a launch failed: the device context may be unusable
+    delete r;
+    return set_error(S->fatal, "server stopped after a failed launch");
+  }
   const dtfe_status_t c = check_params(S->meshes[mesh_id]->m, p);
   if (c != DTFE_OK) {
     delete r;

@@ -154,3 +154,44 @@ def test_kernel_variants_identical_and_autotune(clustered, sd):
         assert table[best]["ms"] == min(t["ms"] for t in table)
     finally:
         m.set_variant(-1)
+
+
+def test_mixed_signed_field_mesh(clustered, sd):
+    """A field mesh (column 3 is a field of either sign, as interpolate_field2grid
+    uses): tets whose vertex values change sign or vanish cannot bound their FP32
+    field value relative to itself and take the FP64 field value.  Pixel values
+    can cross zero, so the error is measured against the map's largest value."""
+    pos4, tetra, _ = clustered
+    f4 = pos4.copy()
+    f4[:, 3] = np.sin(9.0 * pos4[:, 0]) * np.cos(7.0 * pos4[:, 1]) + 0.3 * (pos4[:, 2] - 0.5)
+    with sd.Mesh(f4, tetra, 1.0, sd.MESH_FIELD) as m:
+        for axis in (0, 1):
+            p64 = sd.map_params(80, 1.0, 1.0, (0.5, 0.5, 0.5), 4, 0.0, 31, axis=axis)
+            p32 = sd.map_params(80, 1.0, 1.0, (0.5, 0.5, 0.5), 4, 0.0, 31, axis=axis,
+                                precision=sd.DTFE_MIXED)
+            m64, st64 = m.map(p64)
+            m32, st32 = m.map(p32)
+            assert st32.visits == st64.visits
+            assert (m64 < 0).any() and (m64 > 0).any()
+            assert np.max(np.abs(m32 - m64)) <= MAX_REL * np.max(np.abs(m64))
+
+
+def test_mixed_first_tet_on_hull_slivers(sd):
+    """A jittered lattice: flat tets along the hull faces, rays that start on
+    them, zero-sign cases and perturbations; the mixed walk must still visit the
+    FP64 path's tets and stay within tolerance."""
+    rng = np.random.default_rng(44)
+    g = (np.arange(14) + 0.5) / 14
+    lat = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    lat = lat + rng.normal(scale=0.02 / 14, size=lat.shape)
+    pos4 = np.zeros((len(lat), 4))
+    pos4[:, :3] = lat.astype(np.float32)
+    tetra = sd.triangulate(pos4)
+    with sd.Mesh(pos4, tetra, 1.0) as m:
+        p64 = sd.map_params(56, 1.0, 1.0, (0.5, 0.5, 0.5), 8, 0.0, 3)
+        p32 = sd.map_params(56, 1.0, 1.0, (0.5, 0.5, 0.5), 8, 0.0, 3, precision=sd.DTFE_MIXED)
+        m64, st64 = m.map(p64)
+        m32, st32 = m.map(p32)
+        assert st32.visits == st64.visits
+        assert list(st32.status) == list(st64.status)
+        assert rel_err(m32, m64) <= MAX_REL
