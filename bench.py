@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-load", type=float, default=0.7,
                     help="Poisson arrival rate as a fraction of the measured mixed capacity")
+    ap.add_argument("--serve-quantum", type=int, default=0,
+                    help="rays per serving iteration (0: the library default)")
     return ap.parse_args()
 
 
@@ -497,7 +499,7 @@ def section_serving(args, sd, torch, tri):
                        f"{len(reqs)} requests: random cutout, axis, side in "
                        "{128..2048}, 4-16 samples/pixel",
            "particles_resident": int(sum(cut[h % len(cut)][0] for h in range(args.serve_handles)))}
-    with sd.Server() as srv:
+    with sd.Server(quantum_rays=args.serve_quantum) as srv:
         ids = [srv.add_mesh(m) for m in meshes]
         # warm-up: one small request per cutout touches every handle once
         warm = [srv.submit(i, sd.map_params(32, 1.0, 1.0, (0.5, 0.5, 0.5), 1, seed=1,

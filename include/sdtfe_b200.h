@@ -237,7 +237,8 @@ typedef struct dtfe_server_s *dtfe_server_t;
 typedef struct {
   size_t device_budget;    /* bytes for walk records and maps (0: 3/4 of free memory) */
   int max_active;          /* requests on the GPU at once (0: 64)                     */
-  long long quantum_rays;  /* rays per iteration launch (0: 2^20)                     */
+  long long quantum_rays;  /* rays per iteration launch under light load (0: 2^20);
+                              with a backlog up to 8x this                           */
   int policy;              /* DTFE_SERVE_FAIR or DTFE_SERVE_FIFO                      */
   int variant;             /* mixed kernel variant (-1: default)                      */
 } dtfe_server_config_t;

@@ -248,7 +248,7 @@ dtfe_status_t dtfe_map_device(dtfe_mesh_t h, const dtfe_map_params_t* p, double*
   SDTFE_TRY(check_params(m, p));
   const AxisData& A = m.ax[p->axis];
   const bool ready = A.hull_built && (p->precision == DTFE_FP64 ? A.rec64 != nullptr
-                                                                 : A.rec32 != nullptr &&
+                                                                 : A.rot32 != nullptr &&
                                                                        (m.fp32_exact || A.rec64));
   cudaStream_t s = stream ? (cudaStream_t)stream : m.stream;
   if (!ready) {

@@ -152,8 +152,7 @@ __global__ void k_gradients(const double4* __restrict__ pos, const int4* __restr
 // vertex densities (the mixed walk's barycentric form of the same field).
 __global__ void k_records(const double4* __restrict__ pos, const int4* __restrict__ rows,
                           const double* __restrict__ grad, int nt, int axis,
-                          TetRec64* __restrict__ r64, TetRec32* __restrict__ r32,
-                          TetRot32* __restrict__ rot, int* __restrict__ hz_bits) {
+                          TetRec64* __restrict__ r64, TetRot32* __restrict__ rot) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   const int4 v = rows[2 * (size_t)t];
@@ -177,16 +176,6 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
     r.vid = v;
     r64[t] = r;
   }
-  if (r32) {
-    TetRec32 r;
-    r.xyab = make_float4((float)q[0][0], (float)q[0][1], (float)q[1][0], (float)q[1][1]);
-    r.xycd = make_float4((float)q[2][0], (float)q[2][1], (float)q[3][0], (float)q[3][1]);
-    r.z = make_float4((float)q[0][2], (float)q[1][2], (float)q[2][2], (float)q[3][2]);
-    r.fld = make_float4((float)p[0].w, (float)p[1].w, (float)p[2].w, (float)p[3].w);
-    r.nb = nb;
-    r.aux = v;
-    r32[t] = r;
-  }
   if (rot) {
     // the record of each neighbour as entered from this tet
     const int nbo[4] = {nb.x, nb.y, nb.z, nb.w};
@@ -205,7 +194,6 @@ __global__ void k_records(const double4* __restrict__ pos, const int4* __restric
       const int f = m.x == t ? 0 : (m.y == t ? 1 : (m.z == t ? 2 : (m.w == t ? 3 : -1)));
       nxt[s] = f >= 0 ? 4 * n + f : INT_MIN;
     }
-    atomicMax(hz_bits, __float_as_int(zmax - zmin));  // non-negative: int order = float order
     // extent of the projection, over the float coordinates the walk reads
     float lo[2] = {(float)q[0][0], (float)q[0][1]}, hi[2] = {lo[0], lo[1]};
 #pragma unroll
@@ -385,6 +373,25 @@ dtfe_status_t dmalloc(T** p, size_t count, Mesh* m) {
   return DTFE_OK;
 }
 
+// stream-ordered allocation on the mesh stream (no device-wide synchronisation)
+template <class T>
+dtfe_status_t dmalloc_async(T** p, size_t count, Mesh* m) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  SDTFE_CUDA(cudaMallocAsync((void**)p, count * sizeof(T), m->stream));
+  m->bytes += count * sizeof(T);
+  return DTFE_OK;
+}
+
+template <class T>
+void dfree_async(T*& p, size_t count, Mesh* m) {
+  if (p) {
+    cudaFreeAsync(p, m->stream);
+    m->bytes -= (count ? count : 1) * sizeof(T);
+  }
+  p = nullptr;
+}
+
 template <class T>
 void dfree(T*& p, size_t count, Mesh* m) {
   if (p) {
@@ -496,63 +503,45 @@ dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32) {
   if (axis < 0 || axis > 2) return set_error(DTFE_ERR_INVALID, "axis %d not in 0..2", axis);
   if (!m->grad) return set_error(DTFE_ERR_INVALID, "mesh_records before mesh_gradients");
   AxisData& A = m->ax[axis];
-  const bool need64 = want64 && !A.rec64, need32 = want32 && !A.rec32;
+  const bool need64 = want64 && !A.rec64, need32 = want32 && !A.rot32;
   if (!need64 && !need32) return DTFE_OK;
-  // rotated records address 4*t + F in an int: up to 2^29 - 1 tets
-  const bool need_rot = need32 && m->nt < (1 << 29);
-  // all or nothing: a record array that exists has been built
-  int* hz = nullptr;  // largest tet height, as float bits (non-negative: int order)
+  // the mixed walk's records address 4*t + F in an int: up to 2^29 - 1 tets
+  if (need32 && m->nt >= (1 << 29))
+    return set_error(DTFE_ERR_UNSUPPORTED, "mixed maps of %d tets (at most 2^29 - 1)", m->nt);
+  // all or nothing: a record array that exists has been built; stream-ordered
+  // allocations, so that building records for one mesh does not stall the
+  // device (the serving loop builds and drops them while maps run)
   dtfe_status_t st = DTFE_OK;
-  if (need64) st = dmalloc(&A.rec64, m->nt, m);
-  if (st == DTFE_OK && need32) st = dmalloc(&A.rec32, m->nt, m);
-  if (st == DTFE_OK && need_rot) st = dmalloc(&A.rot32, 4 * (size_t)m->nt, m);
-  cudaError_t e = cudaSuccess;
-  int bits = 0;
+  if (need64) st = dmalloc_async(&A.rec64, m->nt, m);
+  if (st == DTFE_OK && need32) st = dmalloc_async(&A.rot32, 4 * (size_t)m->nt, m);
   if (st == DTFE_OK && m->nt) {
-    if (need_rot) {
-      e = cudaMallocAsync(&hz, sizeof(int), m->stream);
-      if (e == cudaSuccess) e = cudaMemsetAsync(hz, 0, sizeof(int), m->stream);
-    }
-    if (e == cudaSuccess) {
-      k_records<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, axis,
-                                                           need64 ? A.rec64 : nullptr,
-                                                           need32 ? A.rec32 : nullptr,
-                                                           need_rot ? A.rot32 : nullptr, hz);
-      count_launch();
-      e = cudaGetLastError();
-    }
-    if (e == cudaSuccess && need_rot)
-      e = cudaMemcpyAsync(&bits, hz, sizeof(int), cudaMemcpyDeviceToHost, m->stream);
-    if (hz) cudaFreeAsync(hz, m->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    k_records<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, axis,
+                                                         need64 ? A.rec64 : nullptr,
+                                                         need32 ? A.rot32 : nullptr);
+    count_launch();
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
-      st = set_error(e == cudaErrorMemoryAllocation ? DTFE_ERR_NOMEM : DTFE_ERR_CUDA,
-                     "walk records: %s", cudaGetErrorString(e));
+      st = set_error(DTFE_ERR_CUDA, "walk records: %s", cudaGetErrorString(e));
   }
   if (st != DTFE_OK) {
-    if (need64) dfree(A.rec64, m->nt, m);
-    if (need32) dfree(A.rec32, m->nt, m);
-    if (need_rot) dfree(A.rot32, 4 * (size_t)m->nt, m);
+    if (need64) dfree_async(A.rec64, m->nt, m);
+    if (need32) dfree_async(A.rot32, 4 * (size_t)m->nt, m);
     return st;
   }
-  if (need_rot) memcpy(&A.hz_max, &bits, sizeof(float));
-  SDTFE_CUDA(cudaGetLastError());
   return DTFE_OK;
 }
 
 size_t mesh_record_bytes(const Mesh& m, int axis) {
   const AxisData& A = m.ax[axis];
   const size_t nt = (size_t)m.nt;
-  return (A.rec32 ? sizeof(TetRec32) * nt : 0) + (A.rot32 ? 4 * sizeof(TetRot32) * nt : 0) +
-         (A.rec64 ? sizeof(TetRec64) * nt : 0);
+  return (A.rot32 ? 4 * sizeof(TetRot32) * nt : 0) + (A.rec64 ? sizeof(TetRec64) * nt : 0);
 }
 
 size_t mesh_missing_record_bytes(const Mesh& m, int axis, int precision) {
   const AxisData& A = m.ax[axis];
   const size_t nt = (size_t)m.nt;
   size_t b = 0;
-  if (precision == DTFE_MIXED && !A.rec32)
-    b += sizeof(TetRec32) * nt + (m.nt < (1 << 29) ? 4 * sizeof(TetRot32) * nt : 0);
+  if (precision == DTFE_MIXED && !A.rot32) b += 4 * sizeof(TetRot32) * nt;
   // the mixed walk reads FP64 records only when the coordinates are not floats
   const bool want64 = precision == DTFE_FP64 ||
                       (!m.fp32_exact && !(m.flags & DTFE_MESH_NO_FP64_REC));
@@ -560,13 +549,12 @@ size_t mesh_missing_record_bytes(const Mesh& m, int axis, int precision) {
   return b;
 }
 
-// Frees one axis' walk records (the caller has no map of that axis in flight).
+// Frees one axis' walk records (the caller has no map of that axis in flight),
+// ordered on the mesh stream.
 void mesh_drop_records(Mesh* m, int axis) {
   if (axis < 0 || axis > 2) return;
-  if (m->stream) cudaStreamSynchronize(m->stream);
-  dfree(m->ax[axis].rec64, m->nt, m);
-  dfree(m->ax[axis].rec32, m->nt, m);
-  dfree(m->ax[axis].rot32, 4 * (size_t)m->nt, m);
+  dfree_async(m->ax[axis].rec64, m->nt, m);
+  dfree_async(m->ax[axis].rot32, 4 * (size_t)m->nt, m);
 }
 
 dtfe_status_t mesh_hull_mask(Mesh* m, int axis, uint32_t* host_mask_out, int* count_out) {
@@ -685,9 +673,8 @@ void mesh_free(Mesh* m) {
   dfree(m->adj, m->n, m);
   dfree(m->stats, kStatCount, m);
   for (auto& A : m->ax) {
-    dfree(A.rec64, m->nt, m);
-    dfree(A.rec32, m->nt, m);
-    dfree(A.rot32, 4 * (size_t)m->nt, m);
+    dfree_async(A.rec64, m->nt, m);
+    dfree_async(A.rot32, 4 * (size_t)m->nt, m);
     dfree(A.tri, A.n_tri, m);
     dfree(A.tri_rows, 8 * (size_t)A.n_tri, m);
     dfree(A.tri_face, A.n_tri, m);

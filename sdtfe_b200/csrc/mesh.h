@@ -54,9 +54,7 @@ struct AxisData {
   signed char* tri_face = nullptr;  // device, n_tri: the tet face (0..3) under each triangle
   // walk records in this axis' projected frame (built on demand, per precision)
   TetRec64* rec64 = nullptr;
-  TetRec32* rec32 = nullptr;
-  TetRot32* rot32 = nullptr;  // 4 per tet (one per entry face), with rec32
-  float hz_max = 0.f;         // largest z extent of a tet in this frame
+  TetRot32* rot32 = nullptr;  // 4 per tet (one per entry face): the mixed walk's records
 };
 
 struct Mesh {

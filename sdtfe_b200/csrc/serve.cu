@@ -10,9 +10,9 @@
 //      (mesh, axis) pairs are evicted least recently used first; a request
 //      that could never fit is refused with DTFE_ERR_ADMISSION),
 //   4. launches the next iteration: one persistent batch kernel per precision
-//      over a slice of every active request's remaining tiles, about
-//      quantum_rays rays in all (DTFE_SERVE_FAIR: split evenly, smallest
-//      remainder first; DTFE_SERVE_FIFO: oldest first).
+//      over a slice of every active request's remaining tiles, quantum_rays
+//      rays in all, more (up to 8x) while a backlog waits (DTFE_SERVE_FAIR:
+//      split evenly, smallest remainder first; DTFE_SERVE_FIFO: oldest first).
 // Iterations alternate between two streams and two may be in flight, so the
 // next one fills the SMs while the previous one drains.  New requests join at
 // the next iteration: continuous batching, not a queue in front of whole
@@ -281,8 +281,14 @@ void share_tiles(Server* S, std::vector<std::pair<Request*, long long>>* out) {
   for (Request* r : S->active)
     if (r->next_tile < r->tiles) rs.push_back(r);
   if (rs.empty()) return;
-  double budget = (double)S->cfg.quantum_rays;
   auto rest = [](const Request* r) { return (double)(r->tiles - r->next_tile) * r->rays_per_tile; };
+  // The iteration's rays: quantum_rays under light load (short iterations, so
+  // new requests join soon); with a backlog, a quarter of the remaining work,
+  // up to 8x the quantum (fewer, longer iterations: less per-launch cost).
+  double backlog = 0.0;
+  for (const Request* r : rs) backlog += rest(r);
+  const double q = (double)S->cfg.quantum_rays;
+  double budget = std::min(8.0 * q, std::max(q, 0.25 * backlog));
   if (S->cfg.policy == DTFE_SERVE_FAIR)
     std::stable_sort(rs.begin(), rs.end(), [&](Request* a, Request* b) { return rest(a) < rest(b); });
   size_t left = rs.size();
@@ -582,6 +588,12 @@ dtfe_status_t dtfe_server_add_mesh(dtfe_server_t S, dtfe_mesh_t mesh, int* mesh_
   std::lock_guard<std::mutex> lk(S->mu);
   for (dtfe_mesh_t h : S->meshes)
     if (h == mesh) return set_error(DTFE_ERR_INVALID, "mesh already registered");
+  // the projected hulls of all three axes now, so that no request waits for
+  // one (they are small, and their build synchronises the mesh stream)
+  {
+    std::lock_guard<std::mutex> mk(mesh->mu);
+    for (int a = 0; a < 3; ++a) SDTFE_TRY(mesh_hull(&mesh->m, a, nullptr, nullptr));
+  }
   const int id = (int)S->meshes.size();
   S->meshes.push_back(mesh);
   for (int a = 0; a < 3; ++a) {

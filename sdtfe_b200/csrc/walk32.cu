@@ -79,7 +79,7 @@ struct MixConf {
   int exact32;                         // the float coordinates are the doubles
   const TetRot32* __restrict__ rot;    // records per entry face (NULL: general steps only)
   const signed char* __restrict__ tri_face;  // the tet face under each hull triangle
-  const TetRec32* __restrict__ rec32;  // the mesh-order records
+  const int4* __restrict__ rows;       // the mesh's tetra_data rows (vertex ids, neighbours)
   const double4* __restrict__ pos;     // vertices and their densities, original frame
   const double* __restrict__ grad;     // per-tet gradients, original frame
   int axis;                            // projection axis (frame permutation)
@@ -118,37 +118,43 @@ __device__ __forceinline__ void ray_setup(RayState& r, const MixConf& C) {
 struct Verts32 {
   float x[4], y[4];  // absolute (projected frame)
   float z[4];
-  float rho[4];
 };
 
-__device__ __forceinline__ void load32(const TetRec32* __restrict__ R, int t, Verts32& v,
-                                       int4& nb) {
-  const TetRec32* p = R + t;
-  const float4 a = __ldg(&p->xyab), b = __ldg(&p->xycd), z = __ldg(&p->z), f = __ldg(&p->fld);
-  nb = __ldg(&p->nb);
+// The general step sees a tet in the mesh's own vertex order A..D: its record
+// for entry face 3 (ABC) has exactly that slot order (rot_slot(3, k) = k), and
+// the neighbours come from the mesh's tetra_data rows.
+__device__ __forceinline__ const TetRot32* mesh_order(const TetRot32* __restrict__ R, int t) {
+  return R + 4 * (size_t)t + 3;
+}
+
+__device__ __forceinline__ void load32(const TetRot32* __restrict__ R, const int4* __restrict__ rows,
+                                       int t, Verts32& v, int4& nb) {
+  const TetRot32* p = mesh_order(R, t);
+  const float4 a = __ldg(&p->xy01), b = __ldg(&p->xy23), z = __ldg(&p->z);
+  nb = __ldg(&rows[2 * (size_t)t + 1]);
   v.x[0] = a.x; v.y[0] = a.y; v.x[1] = a.z; v.y[1] = a.w;
   v.x[2] = b.x; v.y[2] = b.y; v.x[3] = b.z; v.y[3] = b.w;
   v.z[0] = z.x; v.z[1] = z.y; v.z[2] = z.z; v.z[3] = z.w;
-  v.rho[0] = f.x; v.rho[1] = f.y; v.rho[2] = f.z; v.rho[3] = f.w;
 }
 
 // Exact double coordinates of vertex k of tet t, fetched from memory (the
 // float record when its floats are the doubles, else the FP64 record).
-__device__ __forceinline__ double2 xy64_at(const TetRec32* __restrict__ R32,
+__device__ __forceinline__ double2 xy64_at(const TetRot32* __restrict__ R32,
                                            const TetRec64* __restrict__ R64, int exact32, int t,
                                            int k) {
   if (exact32) {
-    const float4 q = __ldg(k < 2 ? &R32[t].xyab : &R32[t].xycd);
+    const TetRot32* p = mesh_order(R32, t);
+    const float4 q = __ldg(k < 2 ? &p->xy01 : &p->xy23);
     return (k & 1) ? make_double2(q.z, q.w) : make_double2(q.x, q.y);
   }
   return __ldg(&R64[t].xy[k]);
 }
 
-__device__ __forceinline__ double z64_at(const TetRec32* __restrict__ R32,
+__device__ __forceinline__ double z64_at(const TetRot32* __restrict__ R32,
                                          const TetRec64* __restrict__ R64, int exact32, int t,
                                          int k) {
   if (exact32) {
-    const float4 z = __ldg(&R32[t].z);
+    const float4 z = __ldg(&mesh_order(R32, t)->z);
     return (double)sel4(k, z.x, z.y, z.z, z.w);
   }
   const double2 zz = __ldg(k < 2 ? &R64[t].zab : &R64[t].zcd);
@@ -174,7 +180,7 @@ __device__ __forceinline__ double edge_u64_exact(double lz, double ox, double oy
 
 // Slow path: the reference's six signs for tet t, packed 2 bits per edge
 // (0: zero, 1: positive, 2: negative).
-__device__ __noinline__ unsigned exact_signs(const TetRec32* __restrict__ R32,
+__device__ __noinline__ unsigned exact_signs(const TetRot32* __restrict__ R32,
                                              const TetRec64* __restrict__ R64, int exact32,
                                              double lz, int t, double ox, double oy) {
   SDTFE_EDGE_TABLES
@@ -210,7 +216,7 @@ struct Hit32 {
 };
 
 // The filtered test of one tet.  u[] receives the FP32 products (units of lz).
-__device__ __forceinline__ Hit32 tet_test(const TetRec32* __restrict__ R32, const MixConf& C,
+__device__ __forceinline__ Hit32 tet_test(const TetRot32* __restrict__ R32, const MixConf& C,
                                           const RayState& r, int t, const Verts32& v, float u[6],
                                           float* bmax, const unsigned char* __restrict__ lut,
                                           int* fallbacks) {
@@ -269,7 +275,7 @@ __device__ __forceinline__ Hit32 tet_test(const TetRec32* __restrict__ R32, cons
 // Returns a bound on the weights' error (three times the tet's product bound
 // over |sum|): large for a face nearly parallel to the ray.
 __device__ __forceinline__ float crossing(int f, const float u[6], float bmax, const Verts32& v,
-                                          float* dz, float* fv) {
+                                          float* dz) {
   // u: CB=0, AC=1, BA=2, DC=3, BD=4, DA=5
   const float wa = sel4(f, 0.f, -u[3], u[4], u[0]);
   const float wb = sel4(f, u[3], 0.f, u[5], -u[1]);
@@ -279,16 +285,15 @@ __device__ __forceinline__ float crossing(int f, const float u[6], float bmax, c
   const float r = __fdividef(1.f, den);
   const float zb = v.z[1] - v.z[0], zc = v.z[2] - v.z[0], zd = v.z[3] - v.z[0];
   *dz = r * __fmaf_rn(wd, zd, __fmaf_rn(wc, zc, wb * zb));
-  *fv = r * __fmaf_rn(wd, v.rho[3], __fmaf_rn(wc, v.rho[2], __fmaf_rn(wb, v.rho[1], wa * v.rho[0])));
   return 3.f * bmax * fabsf(r);
 }
 
-// Crossing of face f of tet t computed from the exact operands: the
-// reference's FP64 point (face_z64) and the FP64 barycentric field value.
+// z of the crossing of face f of tet t, computed from the exact operands: the
+// reference's FP64 point (face_z64).
 // Used where a crossing is not shared with a neighbouring chord (the ray's
 // entry into and exit from the mesh, a re-entry after a perturbation or a
 // turn-around) and where the FP32 weights are ill-conditioned.
-__device__ __noinline__ double2 exact_crossing(const TetRec32* __restrict__ R32,
+__device__ __noinline__ double exact_crossing(const TetRot32* __restrict__ R32,
                                                const TetRec64* __restrict__ R64, int exact32,
                                                double lz, int t, int f, double ox, double oy) {
   SDTFE_EDGE_TABLES
@@ -302,21 +307,14 @@ __device__ __noinline__ double2 exact_crossing(const TetRec32* __restrict__ R32,
   double u[6];
 #pragma unroll
   for (int e = 0; e < 6; ++e) u[e] = edge_u64_exact(lz, ox, oy, xy[kEdgeP[e]], xy[kEdgeQ[e]]);
-  const double zc = face_z64(f, u, z);
-  const float4 rho = __ldg(&R32[t].fld);
-  const double wa = sel4(f, 0.0, -u[3], u[4], u[0]);
-  const double wb = sel4(f, u[3], 0.0, u[5], -u[1]);
-  const double wc = sel4(f, -u[4], -u[5], 0.0, u[2]);
-  const double wd = sel4(f, -u[0], u[1], -u[2], 0.0);
-  const double fv = (wa * rho.x + wb * rho.y + wc * rho.z + wd * rho.w) / (wa + wb + wc + wd);
-  return make_double2(zc, fv);
+  return face_z64(f, u, z);
 }
 
 // weights error above which a crossing is recomputed in FP64 (2^-12)
 constexpr float kCrossingTol = 2.44140625e-4f;
 
 // The reference's FP64 chord midpoint for the chosen faces (slab-test guard).
-__device__ __noinline__ double midpoint64(const TetRec32* __restrict__ R32,
+__device__ __noinline__ double midpoint64(const TetRot32* __restrict__ R32,
                                           const TetRec64* __restrict__ R64, int exact32, double lz,
                                           int t, int enter, int leave, double ox, double oy) {
   SDTFE_EDGE_TABLES
@@ -339,7 +337,7 @@ __device__ __noinline__ double midpoint64(const TetRec32* __restrict__ R32,
 // field rho_A + grad . (p - A) at the point of the ray line at height zmid,
 // from the mesh's FP64 vertex, density and gradient.
 __device__ __noinline__ double field64(const MixConf& C, int t, double ox, double oy, double zmid) {
-  const int4 v = __ldg(&C.rec32[t].aux);
+  const int4 v = __ldg(&C.rows[2 * (size_t)t]);
   const double4 A = C.pos[v.x];
   double ax, ay, az, gx, gy, gz;
   permute3(C.axis, A.x, A.y, A.z, &ax, &ay, &az);
@@ -354,7 +352,7 @@ __device__ __noinline__ double field64(const MixConf& C, int t, double ox, doubl
 // of one chord is bit-for-bit the entry of the next and the chord lengths
 // telescope.  The slab test compares the float midpoint with a guard band;
 // inside the band the reference's FP64 midpoint decides.
-__device__ __forceinline__ double chord32(const TetRec32* __restrict__ R, const MixConf& C,
+__device__ __forceinline__ double chord32(const TetRot32* __restrict__ R, const MixConf& C,
                                           const RayState& r, int t, int enter, int leave,
                                           double z_in, double z_out, float hz, float e_inout,
                                           int* fallbacks) {
@@ -558,14 +556,14 @@ constexpr int kWalkOn = -1;  // general_step: the walk continues
 // Returns kWalkOn, or the ray's final status.  Kept out of line: it runs on
 // about one step in a hundred and would otherwise crowd the fast loop's
 // registers.
-__device__ __noinline__ int general_step(const TetRec32* __restrict__ R, const MixConf& C,
+__device__ __noinline__ int general_step(const TetRot32* __restrict__ R, const MixConf& C,
                                          uint64_t ray, const unsigned char* __restrict__ lut,
                                          WalkState& w, int* visits, int max_record) {
   RayState& r = w.r;
   const int cur = w.cur;
   int4 nb;
   Verts32 v;
-  load32(R, cur, v, nb);
+  load32(R, C.rows, cur, v, nb);
   float u[6], bmax;
   Hit32 h = tet_test(R, C, r, cur, v, u, &bmax, lut, &w.fallbacks);
   if (!h.ok) return kRayNoExit;
@@ -598,21 +596,19 @@ __device__ __noinline__ int general_step(const TetRec32* __restrict__ R, const M
   // the exact operands where it is not shared (first tet, perturbation,
   // turn-around)
   if (!w.carried || nb_at(nb, enter) != w.prev) {
-    const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, enter, r.ox, r.oy);
-    w.z_in = c.x;
+    w.z_in = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, enter, r.ox, r.oy);
     w.e_in = 0.f;
     ++w.fallbacks;
   }
   // exit crossing: FP32 unless it leaves the mesh (not shared with a
   // neighbouring chord) or is ill-conditioned
-  float dzo, f_unused, e_out = 0.f;
+  float dzo, e_out = 0.f;
   double z_out;
-  const float cond = crossing(leave, u, bmax, v, &dzo, &f_unused);
+  const float cond = crossing(leave, u, bmax, v, &dzo);
   const float hz = fmaxf(fmaxf(fabsf(v.z[1] - v.z[0]), fabsf(v.z[2] - v.z[0])),
                          fabsf(v.z[3] - v.z[0]));
   if (nb_at(nb, leave) == -1 || !(cond <= kCrossingTol)) {
-    const double2 c = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
-    z_out = c.x;
+    z_out = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
     ++w.fallbacks;
   } else {
     z_out = (double)v.z[0] + (double)dzo;
@@ -646,7 +642,7 @@ __device__ __noinline__ int general_step(const TetRec32* __restrict__ R, const M
 // general step.  The first tet is entered through the hull triangle the
 // sample was located in (ft_tri; its face is known from the hull build), at
 // the exact crossing.
-__device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixConf& C, int ft,
+__device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixConf& C, int ft,
                                       int ft_tri, double x, double y, uint64_t ray,
                                       const unsigned char* __restrict__ lut, double* rho_out,
                                       int* crossed_out, int* fallbacks_out, int* visits,
@@ -669,7 +665,7 @@ __device__ __forceinline__ int walk32(const TetRec32* __restrict__ R, const MixC
   int status = kWalkOn;
   if (C.rot && ft_tri >= 0) {  // enter through the located hull face, exactly
     const int F = C.tri_face[ft_tri];
-    z_in = exact_crossing(R, C.rec64, C.exact32, C.lz, ft, F, r.ox, r.oy).x;
+    z_in = exact_crossing(R, C.rec64, C.exact32, C.lz, ft, F, r.ox, r.oy);
     ++fallbacks;
     carried = true;
     ri = 4 * ft + F;
@@ -738,7 +734,7 @@ __device__ __forceinline__ void fill_lut(unsigned char* lut) {
 }
 
 struct MapArgs32 {
-  const TetRec32* __restrict__ rec;
+  const TetRot32* __restrict__ rec;
   const TriRec64* __restrict__ tri;
   int n_tri;
   double* __restrict__ map;
@@ -899,7 +895,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
   }
 }
 
-__global__ void __launch_bounds__(128) k_trace32(const TetRec32* __restrict__ rec,
+__global__ void __launch_bounds__(128) k_trace32(const TetRot32* __restrict__ rec,
                                                  const TriRec64* __restrict__ tri, int n_tri,
                                                  int n_rays, const double* __restrict__ xs,
                                                  const double* __restrict__ ys,
@@ -943,14 +939,15 @@ MixConf mix_conf(const Mesh& m, int axis, double z0, double lz, double dist, uin
   C.exact32 = m.fp32_exact ? 1 : 0;
   C.rot = m.ax[axis].rot32;
   C.tri_face = m.ax[axis].tri_face;
-  C.rec32 = m.ax[axis].rec32;
+  C.rows = m.rows;
   C.pos = m.pos;
   C.grad = m.grad;
   C.axis = axis;
   // A midpoint from FP32-derived crossings is within tol * H of the
-  // reference's (each crossing within tol times its tet's height, H the
-  // largest) plus float rounding of positions of magnitude up to Z.
-  const double H = m.ax[axis].hz_max;
+  // reference's (each crossing within tol times its tet's height, H a bound
+  // on every height: the coordinates' range) plus float rounding of positions
+  // of magnitude up to Z.
+  const double H = 2.0 * m.coord_max;
   const double Z = fmax(fmax(fabs(C.z0d), fabs(C.z1d)), m.coord_max);
   const double G = 64.0 * 5.9604644775390625e-08 * (Z + H) + 2.0 * (double)kCrossingTol * H;
   C.zlo_in = C.z0d + G;
@@ -999,7 +996,7 @@ static_assert(sizeof(kBatch32) / sizeof(kBatch32[0]) == kNumVariants32, "one bat
 // Checks that an axis has what the mixed walk reads.
 dtfe_status_t check_mixed(const Mesh& m, int axis) {
   const AxisData& A = m.ax[axis];
-  if (!A.rec32 || !A.hull_built) return set_error(DTFE_ERR_INVALID, "mixed walk without FP32 records");
+  if (!A.rot32 || !A.hull_built) return set_error(DTFE_ERR_INVALID, "mixed walk without FP32 records");
   if (!m.fp32_exact && !A.rec64)
     return set_error(DTFE_ERR_INVALID, "coordinates are not floats and no FP64 records are kept");
   return DTFE_OK;
@@ -1015,7 +1012,7 @@ dtfe_status_t map_args32(Mesh& m, const MapGeom& g, int vi, double* d_map,
   const AxisData& A = m.ax[g.axis];
   const Variant32& V = kVariants32[vi];
   MapArgs32& a = *out;
-  a.rec = A.rec32;
+  a.rec = A.rot32;
   a.tri = A.tri;
   a.n_tri = A.n_tri;
   a.map = d_map;
@@ -1069,7 +1066,7 @@ dtfe_status_t launch_trace32(Mesh& m, int axis, int n_rays, const double* d_x, c
   const AxisData& A = m.ax[axis];
   MixConf C = mix_conf(m, axis, z0, lz, (dxy / 2.0) / kPerturbMax, seed, max_visits);
   if (n_rays > 0) {
-    k_trace32<<<(n_rays + 127) / 128, 128, 0, s>>>(A.rec32, A.tri, A.n_tri, n_rays, d_x, d_y, C,
+    k_trace32<<<(n_rays + 127) / 128, 128, 0, s>>>(A.rot32, A.tri, A.n_tri, n_rays, d_x, d_y, C,
                                                    4 * A.n_tri + 64, d_rho, d_crossed, d_status,
                                                    d_visits, max_record);
     count_launch();

@@ -1,27 +1,17 @@
-// walk32.cuh - record layouts of the mixed-precision walk.
+// walk32.cuh - record layout of the mixed-precision walk.
 #pragma once
 
 #include <cstdint>
 
 namespace sdtfe {
 
-// 96 B per tet: everything one FP32 walk step reads, in six 16-byte words,
-// vertices in the mesh's own order (A..D).  The general step reads these.
-struct __align__(32) TetRec32 {
-  float4 xyab;  // (x_A, y_A, x_B, y_B) in the projected frame
-  float4 xycd;  // (x_C, y_C, x_D, y_D)
-  float4 z;     // (z_A, z_B, z_C, z_D)
-  float4 fld;   // (rho_A, rho_B, rho_C, rho_D): vertex densities (or field values)
-  int4 nb;      // neighbours across faces BDC, ACD, ADB, ABC (-1: hull)
-  int4 aux;     // vertex ids A..D
-};
-static_assert(sizeof(TetRec32) == 96, "TetRec32 layout");
-
-// 80 B per (tet, entry face): the tet seen by a ray that entered it through
-// face F.  Slots 0..2 hold face F's vertices (in the order the face is listed
-// in: BDC, ACD, ADB, ABC), slot 3 the vertex opposite it.  Record 4*t + F.
-// The fast step reads one of these: the entry face is known, so every slot
-// is fixed and only the exit face (opposite slot 0, 1 or 2) is chosen.
+// 80 B per (tet, entry face), 4 per tet: the mixed walk's records.  Record
+// 4*t + F is the tet seen by a ray that entered it through face F: slots 0..2
+// hold face F's vertices (in the order the face is listed in: BDC, ACD, ADB,
+// ABC), slot 3 the vertex opposite it.  The fast step reads one of these: the
+// entry face is known, so every slot is fixed and only the exit face (opposite
+// slot 0, 1 or 2) is chosen.  Record 4*t + 3 has the vertices in the mesh's
+// own order A..D, which is how the general step reads a tet.
 struct __align__(16) TetRot32 {
   float4 xy01;  // (x0, y0, x1, y1)
   float4 xy23;  // (x2, y2, x3, y3)

@@ -184,9 +184,9 @@ def test_server_admission_and_eviction(sd, cutouts):
     """A small budget forces walk records out (least recently used first);
     results stay exact.  A request that cannot fit even alone is refused."""
     nt = max(m.info().n_tetra for m in cutouts)
-    # room for one mesh's records on one axis (mixed: 96 B per tet in mesh
-    # order plus 4 x 80 B per entry face; FP64: 160 B), plus a few maps
-    budget = nt * (96 + 320 + 160) + 4 * 8 * 128 * 128
+    # room for one mesh's records on one axis (mixed: 4 x 80 B per tet, one
+    # record per entry face; FP64: 160 B), plus a few maps
+    budget = nt * (320 + 160) + 4 * 8 * 128 * 128
     with sd.Server(device_budget=budget, quantum_rays=1 << 15) as srv:
         ids = [srv.add_mesh(m) for m in cutouts]
         reqs = []
