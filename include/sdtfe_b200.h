@@ -109,9 +109,11 @@ const char *dtfe_last_error(void);
 void dtfe_clear_error(void); /* empty the calling thread's last-error message */
 const char *dtfe_status_string(dtfe_status_t s);
 
-/* Upload a mesh and build everything the walks need.  Unless DTFE_MESH_FIELD is
- * set, column 3 of particle_data is ignored and replaced on the device by the
- * DTFE density 4*p_mass / (sum of adjacent |V|) (src/triangulate.c:183-225). */
+/* Upload a mesh and build everything the walks need: densities, gradients, and
+ * the z axis' hull and walk records for the default precision (other axes and
+ * precisions are built on first use).  Unless DTFE_MESH_FIELD is set, column 3
+ * of particle_data is ignored and replaced on the device by the DTFE density
+ * 4*p_mass / (sum of adjacent |V|) (src/triangulate.c:183-225). */
 dtfe_status_t dtfe_mesh_create(const double *particle_data, int n_particles,
                                const int *tetra_data, int n_tetra, float p_mass,
                                unsigned flags, dtfe_mesh_t *out);

@@ -156,10 +156,10 @@ dtfe_status_t dtfe_mesh_create(const double* particle_data, int n_particles, con
   if (s == DTFE_OK && !(flags & DTFE_MESH_FIELD)) s = mesh_density(&m);
   if (s == DTFE_OK) s = mesh_gradients(&m);
   if (s == DTFE_OK) {
-    const bool want64 = !(flags & DTFE_MESH_NO_FP64_REC);
-    s = mesh_records(&m, DTFE_AXIS_Z, want64, !want64);
+    // the z-axis records and hull for the precision maps use by default
+    const int prec = (flags & DTFE_MESH_NO_FP64_REC) ? DTFE_MIXED : dtfe_get_default_precision();
+    s = prepare_axis(m, DTFE_AXIS_Z, prec);
   }
-  if (s == DTFE_OK) s = mesh_hull(&m, DTFE_AXIS_Z, nullptr, nullptr);
   if (s == DTFE_OK) {
     cudaError_t e = cudaStreamSynchronize(m.stream);
     if (e != cudaSuccess) s = set_error(DTFE_ERR_CUDA, "mesh build: %s", cudaGetErrorString(e));

@@ -7,6 +7,7 @@
 // and must not be contracted into fused multiply-adds.
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -373,12 +374,44 @@ dtfe_status_t dmalloc(T** p, size_t count, Mesh* m) {
   return DTFE_OK;
 }
 
-// stream-ordered allocation on the mesh stream (no device-wide synchronisation)
+// The walk records' memory pool of each device: stream-ordered allocation (no
+// device-wide synchronisation when records are built or dropped while maps
+// run), and freed record memory kept for reuse up to an eighth of the device
+// (at most 16 GB) instead of being unmapped and mapped again by every mesh.
+constexpr int kMaxPoolDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_record_pool[kMaxPoolDevices] = {};
+
+dtfe_status_t record_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  SDTFE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxPoolDevices) return set_error(DTFE_ERR_UNSUPPORTED, "device %d", dev);
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_record_pool[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    SDTFE_CUDA(cudaMemPoolCreate(&pool, &props));
+    size_t fr = 0, total = 0;
+    SDTFE_CUDA(cudaMemGetInfo(&fr, &total));
+    uint64_t keep = std::min<uint64_t>(uint64_t(16) << 30, total / 8);
+    SDTFE_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_record_pool[dev] = pool;
+  }
+  *out = g_record_pool[dev];
+  return DTFE_OK;
+}
+
+// stream-ordered allocation from the record pool, on the mesh stream
 template <class T>
 dtfe_status_t dmalloc_async(T** p, size_t count, Mesh* m) {
   *p = nullptr;
   if (count == 0) count = 1;
-  SDTFE_CUDA(cudaMallocAsync((void**)p, count * sizeof(T), m->stream));
+  cudaMemPool_t pool = nullptr;
+  SDTFE_TRY(record_pool(&pool));
+  SDTFE_CUDA(cudaMallocFromPoolAsync((void**)p, count * sizeof(T), pool, m->stream));
   m->bytes += count * sizeof(T);
   return DTFE_OK;
 }
@@ -666,6 +699,11 @@ dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count
 }
 
 void mesh_free(Mesh* m) {
+  // stream-ordered frees first, so that the synchronisation covers them
+  for (auto& A : m->ax) {
+    dfree_async(A.rec64, m->nt, m);
+    dfree_async(A.rot32, 4 * (size_t)m->nt, m);
+  }
   if (m->stream) cudaStreamSynchronize(m->stream);
   dfree(m->pos, m->n, m);
   dfree(m->rows, 2 * (size_t)m->nt, m);
@@ -673,8 +711,6 @@ void mesh_free(Mesh* m) {
   dfree(m->adj, m->n, m);
   dfree(m->stats, kStatCount, m);
   for (auto& A : m->ax) {
-    dfree_async(A.rec64, m->nt, m);
-    dfree_async(A.rot32, 4 * (size_t)m->nt, m);
     dfree(A.tri, A.n_tri, m);
     dfree(A.tri_rows, 8 * (size_t)A.n_tri, m);
     dfree(A.tri_face, A.n_tri, m);

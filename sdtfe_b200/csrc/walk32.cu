@@ -983,6 +983,7 @@ const Variant32 kVariants32[] = {
     {k_map32<256, 2>, 256, 2, 0}, {k_map32<256, 3>, 256, 3, 0}, {k_map32<256, 4>, 256, 4, 0},
     {k_map32<128, 4>, 128, 4, 0}, {k_map32<128, 6>, 128, 6, 0}, {k_map32<256, 2>, 256, 2, 1},
     {k_map32<256, 3>, 256, 3, 1}, {k_map32<128, 8>, 128, 8, 0}, {k_map32<64, 16>, 64, 16, 0},
+    {k_map32<32, 32>, 32, 32, 0},
 };
 constexpr int kNumVariants32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
 constexpr int kDefaultVariant32 = 7;  // (128, 8): the usual winner on B200
@@ -990,7 +991,8 @@ constexpr int kDefaultVariant32 = 7;  // (128, 8): the usual winner on B200
 typedef void (*BatchKernel32)(const BatchJob32*, int, long long, unsigned long long*);
 const BatchKernel32 kBatch32[] = {k_batch32<256, 2>, k_batch32<256, 3>, k_batch32<256, 4>,
                                   k_batch32<128, 4>, k_batch32<128, 6>, k_batch32<256, 2>,
-                                  k_batch32<256, 3>, k_batch32<128, 8>, k_batch32<64, 16>};
+                                  k_batch32<256, 3>, k_batch32<128, 8>, k_batch32<64, 16>,
+                                  k_batch32<32, 32>};
 static_assert(sizeof(kBatch32) / sizeof(kBatch32[0]) == kNumVariants32, "one batch kernel per variant");
 
 // Checks that an axis has what the mixed walk reads.
