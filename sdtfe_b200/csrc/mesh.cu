@@ -404,6 +404,17 @@ dtfe_status_t record_pool(cudaMemPool_t* out) {
   return DTFE_OK;
 }
 
+}  // namespace
+
+void mesh_trim_record_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxPoolDevices) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (g_record_pool[dev]) cudaMemPoolTrimTo(g_record_pool[dev], 0);
+}
+
+namespace {
+
 // stream-ordered allocation from the record pool, on the mesh stream
 template <class T>
 dtfe_status_t dmalloc_async(T** p, size_t count, Mesh* m) {

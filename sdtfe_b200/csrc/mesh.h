@@ -87,6 +87,8 @@ void mesh_drop_records(Mesh* m, int axis);
 // device bytes of one axis' walk records: held now, and still to build for a
 // map of the given precision
 size_t mesh_record_bytes(const Mesh& m, int axis);
+// returns the current device's cached, unused walk-record memory to the system
+void mesh_trim_record_pool();
 size_t mesh_missing_record_bytes(const Mesh& m, int axis, int precision);
 // host_mask (optional) replaces the forward-face test with a caller's bitmap
 // (one 32-bit word per tet, faces in bits 0..3)

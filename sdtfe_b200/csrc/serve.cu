@@ -542,6 +542,10 @@ dtfe_status_t dtfe_server_create(const dtfe_server_config_t* cfg, dtfe_server_t*
   };
   cuda(cudaGetDevice(&S->device), "device");
   if (st == DTFE_OK && S->cfg.device_budget == 0) {
+    // memory the record pool keeps for reuse is free for this budget: the
+    // server's record builds draw on the same pool
+    cuda(cudaDeviceSynchronize(), "synchronise");
+    mesh_trim_record_pool();
     size_t fr = 0, total = 0;
     cuda(cudaMemGetInfo(&fr, &total), "memory info");
     S->cfg.device_budget = fr / 4 * 3;
