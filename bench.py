@@ -306,6 +306,23 @@ def read_ncu_traffic(kernel, n_tets):
         return None
 
 
+def slowest_rank_ms(total_ms, dist, device):
+    """The job's device time over replicas: the slowest rank's (max over ranks;
+    every rank calls this, in the same order)."""
+    if dist is None:
+        return total_ms
+    import torch
+
+    tt = torch.tensor([total_ms], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_rays_per_s(rays_per_map, steps, world, total_ms):
+    """Whole-job rays/s: every rank maps its own copy of the workload."""
+    return rays_per_map * steps * world / (total_ms / 1e3)
+
+
 def plan_sections(args):
     """Qhull for the main workload and the sections, in a process pool, before
     any CUDA call (sections run at N=1 only)."""
@@ -604,13 +621,8 @@ def run_ours(args, pre=None):
     clk = clocks.stop()
     step_ms = np.array([a.elapsed_time(b) for a, b in ev])
     st = mesh.last_stats()
-    total_ms = float(step_ms.sum())
-    if dist:
-        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    rays_all = spec.rays * args.steps * world
-    value = rays_all / (total_ms / 1e3)
+    total_ms = slowest_rank_ms(float(step_ms.sum()), dist, dev)
+    value = replica_rays_per_s(spec.rays, args.steps, world, total_ms)
     mixed_map = d_map.cpu().numpy().copy()
 
     # the plain FP64 path on the same map, and the mixed map's error against it
