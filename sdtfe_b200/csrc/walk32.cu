@@ -720,7 +720,9 @@ __device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixC
     carried = w.carried;
     if (status != kWalkOn) break;
   }
-  *crossed_out = crossed;
+  // as the reference (and walk64): a ray that fails reports no crossings, so
+  // that the pixel mean leaves it out
+  *crossed_out = status == kRayOk ? crossed : 0;
   *rho_out = status == kRayOk ? sum : 0.0;
   *fallbacks_out = fallbacks;
   return status;

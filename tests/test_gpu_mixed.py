@@ -195,3 +195,40 @@ def test_mixed_first_tet_on_hull_slivers(sd):
         assert st32.visits == st64.visits
         assert list(st32.status) == list(st64.status)
         assert rel_err(m32, m64) <= MAX_REL
+
+
+def test_mixed_corrupt_links_end_like_fp64(golden, sd):
+    """Neighbour links that do not point back (a 2-cycle): the per-entry-face
+    records mark such neighbours, the general step follows the mesh rows, and
+    the visit budget ends each ray with the FP64 path's status and count."""
+    s = golden_set(golden, "uniform")
+    tet = s["tetra"].copy()
+    inner = tet[:, 4:] >= 0
+    tet[:, 4:][inner] = (np.arange(len(tet))[:, None].repeat(4, 1) % 2)[inner]
+    xs = np.linspace(0.2, 0.8, 9)
+    ys = np.linspace(0.3, 0.7, 9)
+    with sd.Mesh(s["pos4"], tet, 1.0) as m:
+        p64 = sd.map_params(8, 1.0, 1.0, (0.5, 0.5, 0.5), 1, 0.0, 1, max_visits=500)
+        p32 = sd.map_params(8, 1.0, 1.0, (0.5, 0.5, 0.5), 1, 0.0, 1, max_visits=500,
+                            precision=sd.DTFE_MIXED)
+        r64, c64, s64, _ = m.trace(p64, xs, ys, 0.0, 1.0, 0.04)
+        r32, c32, s32, _ = m.trace(p32, xs, ys, 0.0, 1.0, 0.04)
+    assert np.array_equal(s32, s64) and np.array_equal(c32, c64)
+    assert (s32 != 0).all()
+
+
+@pytest.mark.parametrize("G,S", [(1, 300), (5, 257), (3, 33)])
+def test_more_samples_than_threads(golden, sd, oracle, G, S):
+    """A pixel with more samples than a tile has threads (the tile walks them
+    in several passes) and maps of one or a few pixels: FP64 equals the
+    oracle, mixed stays within tolerance of FP64."""
+    s = golden_set(golden, "clustered")
+    prep = oracle.prepare(s["pos4"], s["tetra"], 1.0)
+    want = oracle.map(prep, G, 0.5, 1.0, (0.5, 0.5, 0.5), S, 0.0, 61)
+    with sd.Mesh(s["pos4"], s["tetra"], 1.0) as m:
+        m64, st64 = m.map(sd.map_params(G, 0.5, 1.0, (0.5, 0.5, 0.5), S, 0.0, 61))
+        m32, st32 = m.map(sd.map_params(G, 0.5, 1.0, (0.5, 0.5, 0.5), S, 0.0, 61,
+                                        precision=sd.DTFE_MIXED))
+    assert np.array_equal(m64, want)
+    assert st64.rays == G * G * S and st32.visits == st64.visits
+    assert rel_err(m32, m64) <= MAX_REL
