@@ -31,6 +31,8 @@ struct dtfe_batch_s {
   int grid = 0, block = 0;
   void* d_jobs = nullptr;
   size_t d_jobs_bytes = 0;
+  void* d_loc = nullptr;  // mixed: one tile location per queued tile
+  size_t d_loc_bytes = 0;
   unsigned long long* d_queue = nullptr;
   unsigned long long* d_stats = nullptr;  // kStatCount per job, caller's order
   cudaStream_t stream = nullptr;
@@ -53,6 +55,7 @@ void free_batch(dtfe_batch_s* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graph(b);
   if (b->d_jobs) cudaFree(b->d_jobs);
+  if (b->d_loc) cudaFree(b->d_loc);
   if (b->d_queue) cudaFree(b->d_queue);
   if (b->d_stats) cudaFree(b->d_stats);
   if (b->ev0) cudaEventDestroy(b->ev0);
@@ -91,6 +94,16 @@ dtfe_status_t plan(dtfe_batch_s* b) {
   if (bytes)
     SDTFE_CUDA(cudaMemcpyAsync(b->d_jobs, b->plan.jobs.data(), bytes, cudaMemcpyHostToDevice,
                                b->stream));
+  const size_t loc_bytes =
+      b->precision == DTFE_MIXED ? kLocBytes * (size_t)b->plan.total_tiles : 0;
+  if (loc_bytes > b->d_loc_bytes) {
+    SDTFE_CUDA(cudaStreamSynchronize(b->stream));  // no launch still reads the old buffer
+    if (b->d_loc) SDTFE_CUDA(cudaFree(b->d_loc));
+    b->d_loc = nullptr;
+    b->d_loc_bytes = 0;
+    SDTFE_CUDA(cudaMalloc(&b->d_loc, loc_bytes));
+    b->d_loc_bytes = loc_bytes;
+  }
   SDTFE_CUDA(cudaStreamSynchronize(b->stream));  // the host table is reused by the next plan
   drop_graph(b);
   return DTFE_OK;
@@ -103,7 +116,8 @@ dtfe_status_t enqueue(dtfe_batch_s* b, cudaStream_t s) {
   if (b->flags & DTFE_BATCH_ZERO_MAPS)
     for (const auto& j : b->jobs)
       SDTFE_CUDA(cudaMemsetAsync(j.d_map, 0, sizeof(double) * (size_t)j.params.grid_dim * j.params.grid_dim, s));
-  if (b->precision == DTFE_MIXED) return launch_batch32(b->plan, b->d_jobs, b->d_queue, b->grid, s);
+  if (b->precision == DTFE_MIXED)
+    return launch_batch32(b->plan, b->d_jobs, b->d_queue, b->d_loc, b->grid, s);
   return launch_batch64(b->plan, b->d_jobs, b->d_queue, b->grid, s);
 }
 
@@ -125,7 +139,8 @@ dtfe_status_t launch(dtfe_batch_s* b, cudaStream_t s) {
     }
     SDTFE_CUDA(cudaEventRecord(b->ev0, s));
     SDTFE_CUDA(cudaGraphLaunch(b->exec, s));
-    count_launch(b->plan.n_jobs ? 1 : 0);  // the graph's kernel node
+    // the graph's kernel nodes: the mixed path's tile locations, then the walk
+    count_launch(b->plan.n_jobs ? (b->precision == DTFE_MIXED ? 2 : 1) : 0);
   } else {
     SDTFE_CUDA(cudaEventRecord(b->ev0, s));
     SDTFE_TRY(enqueue(b, s));

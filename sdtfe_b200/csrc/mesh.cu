@@ -406,6 +406,20 @@ dtfe_status_t record_pool(cudaMemPool_t* out) {
 
 }  // namespace
 
+// Per-call device scratch, stream-ordered from the record pool (whose freed
+// memory is kept for reuse, so a map's scratch costs no mapping).
+dtfe_status_t scratch_alloc_async(void** p, size_t bytes, cudaStream_t s) {
+  *p = nullptr;
+  cudaMemPool_t pool = nullptr;
+  SDTFE_TRY(record_pool(&pool));
+  SDTFE_CUDA(cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s));
+  return DTFE_OK;
+}
+
+void scratch_free_async(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
 void mesh_trim_record_pool() {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxPoolDevices) return;

@@ -89,6 +89,9 @@ void mesh_drop_records(Mesh* m, int axis);
 size_t mesh_record_bytes(const Mesh& m, int axis);
 // returns the current device's cached, unused walk-record memory to the system
 void mesh_trim_record_pool();
+// per-call device scratch, stream-ordered on s from the walk-record pool
+dtfe_status_t scratch_alloc_async(void** p, size_t bytes, cudaStream_t s);
+void scratch_free_async(void* p, cudaStream_t s);
 size_t mesh_missing_record_bytes(const Mesh& m, int axis, int precision);
 // host_mask (optional) replaces the forward-face test with a caller's bitmap
 // (one 32-bit word per tet, faces in bits 0..3)
@@ -169,8 +172,11 @@ dtfe_status_t batch_grid32(int variant, size_t smem, int* grid, int* block);
 // d_jobs holds plan.jobs; d_queue is a zeroed counter
 dtfe_status_t launch_batch64(const BatchPlan& plan, const void* d_jobs, unsigned long long* d_queue,
                              int grid, cudaStream_t s);
+// (mixed) d_loc: room for plan.total_tiles tile locations (kLocBytes each)
 dtfe_status_t launch_batch32(const BatchPlan& plan, const void* d_jobs, unsigned long long* d_queue,
-                             int grid, cudaStream_t s);
+                             void* d_loc, int grid, cudaStream_t s);
+// bytes of one tile's shared point-location result
+constexpr size_t kLocBytes = 8;
 int default_variant32();
 
 }  // namespace sdtfe

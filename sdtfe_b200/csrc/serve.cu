@@ -74,6 +74,8 @@ struct Slot {
   unsigned char* h_jobs = nullptr;  // pinned
   void* d_jobs = nullptr;
   size_t cap = 0;
+  void* d_loc = nullptr;  // mixed tiles' shared point locations
+  size_t loc_cap = 0;
   unsigned long long* d_queue = nullptr;  // two counters: mixed, FP64
 };
 
@@ -335,6 +337,15 @@ dtfe_status_t launch_iteration(Server* S, Slot& sl, const std::vector<std::pair<
     SDTFE_CUDA(cudaMalloc(&sl.d_jobs, cap));
     sl.cap = cap;
   }
+  // the slot's previous iteration has finished: its buffers can be replaced
+  const size_t loc_bytes = kLocBytes * (size_t)plans[0].total_tiles;
+  if (loc_bytes > sl.loc_cap) {
+    if (sl.d_loc) cudaFree(sl.d_loc);
+    sl.d_loc = nullptr;
+    sl.loc_cap = 0;
+    SDTFE_CUDA(cudaMalloc(&sl.d_loc, loc_bytes * 2));
+    sl.loc_cap = loc_bytes * 2;
+  }
   if (!plans[0].jobs.empty()) memcpy(sl.h_jobs, plans[0].jobs.data(), plans[0].jobs.size());
   if (!plans[1].jobs.empty()) memcpy(sl.h_jobs + b0, plans[1].jobs.data(), plans[1].jobs.size());
   SDTFE_CUDA(cudaMemcpyAsync(sl.d_jobs, sl.h_jobs, bytes, cudaMemcpyHostToDevice, s));
@@ -343,7 +354,7 @@ dtfe_status_t launch_iteration(Server* S, Slot& sl, const std::vector<std::pair<
   if (plans[0].n_jobs) {
     int grid = 0, block = 0;
     SDTFE_TRY(batch_grid32(plans[0].variant, plans[0].smem, &grid, &block));
-    SDTFE_TRY(launch_batch32(plans[0], dj, sl.d_queue, grid, s));
+    SDTFE_TRY(launch_batch32(plans[0], dj, sl.d_queue, sl.d_loc, grid, s));
     ++S->st.iterations;
   }
   if (plans[1].n_jobs) {
@@ -508,6 +519,7 @@ void free_server(Server* S) {
     if (sl.ev) cudaEventDestroy(sl.ev);
     if (sl.h_jobs) cudaFreeHost(sl.h_jobs);
     if (sl.d_jobs) cudaFree(sl.d_jobs);
+    if (sl.d_loc) cudaFree(sl.d_loc);
     if (sl.d_queue) cudaFree(sl.d_queue);
   }
   if (S->d_stats) cudaFree(S->d_stats);

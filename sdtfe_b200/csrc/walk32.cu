@@ -794,11 +794,42 @@ __device__ __forceinline__ void add_stats32(unsigned long long* stats, bool acti
   }
 }
 
+// The rectangle holding every sample position of a tile.  A ray's position
+// is x(col) + u * scale with u in [0, 1), x(col) the expression below (the
+// same as the rays'); each is monotone in col and u, so the tile's positions
+// lie in [x(tx0), x(c1) + scale], and the same for y.
+__device__ __forceinline__ void tile_rect(const MapArgs32& a, int tile, double* xlo, double* xhi,
+                                          double* ylo, double* yhi) {
+  const int tx0 = (tile % a.tiles_x) * a.TW, ty0 = (tile / a.tiles_x) * a.TH;
+  const int c1 = min(tx0 + a.TW, a.G) - 1, r1 = min(ty0 + a.TH, a.G) - 1;
+  *xlo = tx0 * a.dxy + a.offx - a.soff;
+  *xhi = (c1 * a.dxy + a.offx - a.soff) + a.scale;
+  *ylo = ty0 * a.dxy + a.offy - a.soff;
+  *yhi = (r1 * a.dxy + a.offy - a.soff) + a.scale;
+}
+
+// A tile's shared point location (locate_region), packed for the map kernel:
+// (kind | steps << 2, start triangle).
+__device__ __forceinline__ int2 tile_location(const MapArgs32& a, int tile) {
+  int kind = kLocMiss, start = -1, steps = 0;
+  if (a.n_tri > 0) {
+    double xlo, xhi, ylo, yhi;
+    tile_rect(a, tile, &xlo, &xhi, &ylo, &yhi);
+    kind = locate_region(a.tri, xlo, xhi, ylo, yhi, a.loc_budget, &start, &steps);
+  }
+  return make_int2(kind | (steps << 2), start);
+}
+
 // One tile of one map: TW x TH pixels x S samples on BLOCK threads, one ray
 // per (pixel, sample), the S rays of a pixel in neighbouring lanes; the pixel
 // means are formed in sample order from shared memory (src/dtfe.c:615-645).
+// Point location (src/dtfe.c:518-552) starts from the tile's shared walk
+// (*loc, from tile_location): a ray resumes the walk from triangle 0 where
+// the tile's rectangle straddled a test, so it reaches exactly the triangle
+// and status of its own walk.
 template <int BLOCK>
 __device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
+                                           const int2* __restrict__ loc,
                                            const unsigned char* __restrict__ lut, double* s_val,
                                            unsigned char* s_ok) {
   const int P = a.TW * a.TH;
@@ -817,7 +848,15 @@ __device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
       const double yt = y + sdtfe_sample_u01(a.C.seed, (uint64_t)p, (uint32_t)s, 1) * a.scale;
       const uint64_t rid = (uint64_t)p * (uint64_t)a.S + (uint64_t)s;
       int ft = -1, ft_tri = -1;
-      if (a.n_tri > 0) ft = locate64(a.tri, 0, xt, yt, a.loc_budget, &status, &ft_tri);
+      const int2 l = __ldg(loc);
+      const int lk = l.x & 3;
+      if (lk == kLocFound) {
+        ft = __ldg(&a.tri[l.y].nb.w);
+        ft_tri = l.y;
+        status = kRayOk;
+      } else if (lk == kLocResume) {
+        ft = locate64(a.tri, l.y, xt, yt, a.loc_budget - (l.x >> 2), &status, &ft_tri);
+      }  // else every ray of the tile leaves the hull (or there is none): a miss
       if (ft >= 0)
         status = walk32(a.rec, a.C, ft, ft_tri, xt, yt, rid, lut, &v, &crossed, &fb, nullptr, 0);
       if (status != kRayOk) v = 0.0;
@@ -849,13 +888,22 @@ __device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
 // register budget) are compile-time; the autotuner picks among the
 // instantiations.
 template <int BLOCK, int MINB>
-__global__ void __launch_bounds__(BLOCK, MINB) k_map32(const __grid_constant__ MapArgs32 a) {
+__global__ void __launch_bounds__(BLOCK, MINB)
+    k_map32(const __grid_constant__ MapArgs32 a, const int2* __restrict__ loc) {
   extern __shared__ double s_val32[];  // P*S doubles, then P*S success bytes
   __shared__ unsigned char s_lut[kLutBytes];
   fill_lut(s_lut);
   __syncthreads();
   unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + a.TW * a.TH * a.S);
-  map_tile32<BLOCK>(a, blockIdx.x, s_lut, s_val32, s_ok);
+  map_tile32<BLOCK>(a, blockIdx.x, loc + blockIdx.x, s_lut, s_val32, s_ok);
+}
+
+// Every tile's shared point location, one thread per tile, before the map
+// kernel: the walk from triangle 0 runs once per tile, off the rays' path.
+__global__ void __launch_bounds__(128) k_locate_map32(const __grid_constant__ MapArgs32 a,
+                                                      int n_tiles, int2* __restrict__ loc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n_tiles) loc[t] = tile_location(a, t);
 }
 
 // Persistent batch: the blocks of one launch pull tiles from a device counter
@@ -879,10 +927,25 @@ __device__ __forceinline__ void claim_tile(const BatchJob32* __restrict__ jobs, 
   *job = lo;
 }
 
+// The same for the global tiles of a batch (loc indexed by global tile).
+__global__ void __launch_bounds__(128) k_locate_batch32(const BatchJob32* __restrict__ jobs,
+                                                        int n_jobs, long long total_tiles,
+                                                        int2* __restrict__ loc) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= total_tiles) return;
+  int lo = 0, hi = n_jobs - 1;  // last job whose first tile <= t
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (jobs[mid].first <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  loc[t] = tile_location(jobs[lo].args, jobs[lo].tile0 + (int)(t - jobs[lo].first));
+}
+
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB)
     k_batch32(const BatchJob32* __restrict__ jobs, int n_jobs, long long total_tiles,
-              unsigned long long* __restrict__ queue) {
+              unsigned long long* __restrict__ queue, const int2* __restrict__ loc) {
   extern __shared__ double s_val32[];
   __shared__ unsigned char s_lut[kLutBytes];
   __shared__ MapArgs32 s_args;
@@ -908,7 +971,8 @@ __global__ void __launch_bounds__(BLOCK, MINB)
       __syncthreads();
     }
     unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + s_args.TW * s_args.TH * s_args.S);
-    map_tile32<BLOCK>(s_args, jobs[j].tile0 + (int)(tile - jobs[j].first), s_lut, s_val32, s_ok);
+    map_tile32<BLOCK>(s_args, jobs[j].tile0 + (int)(tile - jobs[j].first), loc + tile, s_lut,
+                      s_val32, s_ok);
     __syncthreads();  // s_val, s_args and the claimed slot are reused next
   }
 }
@@ -990,7 +1054,8 @@ void tile_shape32(int threads, int S, int wide, int* TW, int* TH) {
   *TH = th < 1 ? 1 : th;
 }
 
-typedef void (*MapKernel32)(const MapArgs32);
+static_assert(sizeof(int2) == kLocBytes, "tile location layout");
+typedef void (*MapKernel32)(const MapArgs32, const int2*);
 
 struct Variant32 {
   MapKernel32 kernel;
@@ -1006,7 +1071,7 @@ const Variant32 kVariants32[] = {
 constexpr int kNumVariants32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
 constexpr int kDefaultVariant32 = 7;  // (128, 8): the usual winner on B200
 
-typedef void (*BatchKernel32)(const BatchJob32*, int, long long, unsigned long long*);
+typedef void (*BatchKernel32)(const BatchJob32*, int, long long, unsigned long long*, const int2*);
 const BatchKernel32 kBatch32[] = {k_batch32<256, 2>, k_batch32<256, 3>, k_batch32<256, 4>,
                                   k_batch32<128, 4>, k_batch32<128, 6>, k_batch32<256, 2>,
                                   k_batch32<256, 3>, k_batch32<128, 8>, k_batch32<64, 16>,
@@ -1047,6 +1112,10 @@ dtfe_status_t map_args32(Mesh& m, const MapGeom& g, int vi, double* d_map,
   a.scale = g.scale;
   a.soff = g.soff;
   a.C = mix_conf(m, g.axis, g.offz, g.lz, g.dist, g.seed, g.max_visits);
+  // the location walk's budget; tile_location packs its steps as steps << 2
+  if (A.n_tri >= (1 << 27))
+    return set_error(DTFE_ERR_UNSUPPORTED, "mixed maps over %d hull triangles (at most 2^27 - 1)",
+                     A.n_tri);
   a.loc_budget = 4 * A.n_tri + 64;
   a.stats = stats;
   a.ray_rho = ray_rho;
@@ -1069,10 +1138,17 @@ dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
     SDTFE_CUDA(cudaFuncSetAttribute(V.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long blocks = (long long)a.tiles_x * tiles_y;
   SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
+  void* loc = nullptr;
+  SDTFE_TRY(scratch_alloc_async(&loc, kLocBytes * (size_t)blocks, s));
   SDTFE_CUDA(cudaEventRecord(m.ev0, s));
-  V.kernel<<<(unsigned)blocks, V.block, smem, s>>>(a);
+  k_locate_map32<<<(unsigned)((blocks + 127) / 128), 128, 0, s>>>(a, (int)blocks,
+                                                                  static_cast<int2*>(loc));
   count_launch();
-  SDTFE_CUDA(cudaGetLastError());
+  V.kernel<<<(unsigned)blocks, V.block, smem, s>>>(a, static_cast<const int2*>(loc));
+  count_launch();
+  const cudaError_t e = cudaGetLastError();
+  scratch_free_async(loc, s);
+  SDTFE_CUDA(e);
   SDTFE_CUDA(cudaEventRecord(m.ev1, s));
   m.timed = true;
   return DTFE_OK;
@@ -1157,14 +1233,18 @@ dtfe_status_t batch_grid32(int variant, size_t smem, int* grid, int* block) {
 }
 
 dtfe_status_t launch_batch32(const BatchPlan& plan, const void* d_jobs, unsigned long long* d_queue,
-                             int grid, cudaStream_t s) {
+                             void* d_loc, int grid, cudaStream_t s) {
   if (plan.n_jobs == 0) return DTFE_OK;
   const int vi = pick_variant32(plan.variant);
   if (plan.smem > 40 * 1024)
     SDTFE_CUDA(cudaFuncSetAttribute(kBatch32[vi], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)plan.smem));
+  const BatchJob32* jobs = static_cast<const BatchJob32*>(d_jobs);
+  k_locate_batch32<<<(unsigned)((plan.total_tiles + 127) / 128), 128, 0, s>>>(
+      jobs, plan.n_jobs, plan.total_tiles, static_cast<int2*>(d_loc));
+  count_launch();
   kBatch32[vi]<<<grid, kVariants32[vi].block, plan.smem, s>>>(
-      static_cast<const BatchJob32*>(d_jobs), plan.n_jobs, plan.total_tiles, d_queue);
+      jobs, plan.n_jobs, plan.total_tiles, d_queue, static_cast<const int2*>(d_loc));
   count_launch();
   SDTFE_CUDA(cudaGetLastError());
   return DTFE_OK;

@@ -189,6 +189,99 @@ __device__ __forceinline__ int locate64(const TriRec64* __restrict__ tri, int st
   return -1;
 }
 
+// One of locate64's edge tests (edge o->p, opposite vertex opp: s_in * s_q <
+// 0) decided for every query point of the rectangle [xlo, xhi] x [ylo, yhi]
+// at once: 1 when it holds for all of them, 0 when it fails for all, -1 when
+// the outcome may differ inside.  s_in is the reference's own value.  The
+// FP64 s_q = (qx - o.x) dy - (qy - o.y) dx (dy, dx the rounded edge
+// differences) is within 3.0001 u M(q) of the linear form L(q) = (qx - o.x) dy
+// - (qy - o.y) dx, M(q) = |qx - o.x| |dy| + |qy - o.y| |dx| (u = 2^-53; the
+// operations are not contracted).  L and M take their extremes at the
+// corners, so every s_q lies within 6.0002 u max M of the corners' FP64
+// values; 16 u covers that and the rounding of the bound, and 2^-1000 any
+// underflow.  The product s_in * s_q is then of one sign for all queries,
+// and well clear of underflow to zero.
+__host__ __device__ inline int edge_region(double2 o, double2 p, double2 opp, double xlo,
+                                           double xhi, double ylo, double yhi) {
+  const double s_in = (opp.x - o.x) * (p.y - o.y) - (opp.y - o.y) * (p.x - o.x);
+  if (s_in == 0.0) return 0;  // the product is (signed) zero for every query
+  const double dy = p.y - o.y, dx = p.x - o.x;
+  const double qx[4] = {xlo, xhi, xlo, xhi}, qy[4] = {ylo, ylo, yhi, yhi};
+  double lo = 0.0, hi = 0.0, mag = 0.0;
+  for (int k = 0; k < 4; ++k) {
+    const double tx = qx[k] - o.x, ty = qy[k] - o.y;
+    const double s = tx * dy - ty * dx;
+    lo = k == 0 ? s : (s < lo ? s : lo);
+    hi = k == 0 ? s : (s > hi ? s : hi);
+    const double m = (tx < 0.0 ? -tx : tx) * (dy < 0.0 ? -dy : dy) +
+                     (ty < 0.0 ? -ty : ty) * (dx < 0.0 ? -dx : dx);
+    mag = m > mag ? m : mag;
+  }
+  const double err = 16.0 * 0x1p-53 * mag + 0x1p-1000;
+  const double a_in = s_in < 0.0 ? -s_in : s_in;
+  if (lo > err) {  // s_q > 0 throughout
+    if (a_in * (lo - err) < 0x1p-1000) return -1;
+    return s_in < 0.0 ? 1 : 0;
+  }
+  if (hi < -err) {  // s_q < 0 throughout
+    if (a_in * (-err - hi) < 0x1p-1000) return -1;
+    return s_in > 0.0 ? 1 : 0;
+  }
+  return -1;
+}
+
+enum LocKind : int {
+  kLocResume = 0,  // each query continues locate64 from *start with max_steps - *steps
+  kLocFound = 1,   // every query's walk ends in triangle *start
+  kLocMiss = 2,    // every query's walk leaves the hull
+};
+
+// The reference's location walk from triangle 0 (locate64), run once for a
+// whole rectangle of query points while each edge test has one outcome for
+// all of them.  Where the rectangle straddles a test, the walk stops and each
+// query resumes it on its own at that triangle, with the steps taken so far
+// counted against its budget: every query then makes exactly the moves, and
+// ends with exactly the result, of its own walk from triangle 0.
+__host__ __device__ inline int locate_region(const TriRec64* tri, double xlo, double xhi,
+                                             double ylo, double yhi, int max_steps, int* start,
+                                             int* steps_out) {
+  int cur = 0, steps = 0;
+  for (;;) {
+    if (steps >= max_steps) break;  // each query's next step exceeds its budget
+    const TriRec64& t = tri[cur];
+    int nx = -1;
+    int r = edge_region(t.a, t.b, t.c, xlo, xhi, ylo, yhi);  // edge a-b
+    if (r == 1) {
+      nx = t.nb.z;
+    } else if (r == 0) {
+      r = edge_region(t.b, t.c, t.a, xlo, xhi, ylo, yhi);  // edge b-c
+      if (r == 1) {
+        nx = t.nb.x;
+      } else if (r == 0) {
+        r = edge_region(t.c, t.a, t.b, xlo, xhi, ylo, yhi);  // edge c-a
+        if (r == 1) {
+          nx = t.nb.y;
+        } else if (r == 0) {
+          *start = cur;
+          *steps_out = steps;
+          return kLocFound;
+        }
+      }
+    }
+    if (r < 0) break;
+    ++steps;
+    if (nx == -1) {
+      *start = -1;
+      *steps_out = steps;
+      return kLocMiss;
+    }
+    cur = nx;
+  }
+  *start = cur;
+  *steps_out = steps;
+  return kLocResume;
+}
+
 // ---------------------------------------------------------------------------
 // Accumulators: what a walk does with each crossed tet.
 
