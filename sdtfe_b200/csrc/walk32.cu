@@ -1138,9 +1138,9 @@ dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
     SDTFE_CUDA(cudaFuncSetAttribute(V.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long blocks = (long long)a.tiles_x * tiles_y;
   SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
-  void* loc = nullptr;
-  SDTFE_TRY(scratch_alloc_async(&loc, kLocBytes * (size_t)blocks, s));
   SDTFE_CUDA(cudaEventRecord(m.ev0, s));
+  void* loc = nullptr;  // each tile's shared point location
+  SDTFE_TRY(scratch_alloc_async(&loc, kLocBytes * (size_t)blocks, s));
   k_locate_map32<<<(unsigned)((blocks + 127) / 128), 128, 0, s>>>(a, (int)blocks,
                                                                   static_cast<int2*>(loc));
   count_launch();
