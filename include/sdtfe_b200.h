@@ -80,7 +80,7 @@ typedef struct {
   unsigned long long visits;                       /* tets crossed, summed over rays */
   unsigned long long status[DTFE_N_RAY_STATUS];    /* rays per dtfe_ray_status_t     */
   unsigned long long fp64_fallbacks;               /* MIXED: guarded FP64 re-tests   */
-  double walk_ms;                                  /* device time of the walk kernel */
+  double walk_ms;                 /* device time of the map's kernels (walk, and tile location) */
 } dtfe_map_stats_t;
 
 typedef struct {
