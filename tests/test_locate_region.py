@@ -150,3 +150,50 @@ def test_tile_location_keeps_the_step_budget(lr, oracle, meshes):
         kinds, bad = _check_mesh(lr, oracle, pos4, tet, rng, n_tiles=40, per_tile=8,
                                  budget=budget)
         assert not bad, (name, budget, bad[:3])
+
+
+def test_tile_location_on_vertices_and_edges(lr, oracle, meshes):
+    """Rectangles with corners exactly on lattice vertices (queries on edge
+    lines, where s_q is exactly zero), zero-width rectangles, and queries at
+    the corners and on the sides."""
+    name, pos4, tet = meshes[3]  # the exact lattice
+    prep = oracle.prepare(pos4, tet, 1.0)
+    tri, pos = prep["tri"], prep["pos"]
+    P = pos[:, :2]
+    abc = np.ascontiguousarray(np.stack([P[tri[:, 0]], P[tri[:, 1]], P[tri[:, 2]]], 1).reshape(-1, 6))
+    nb = np.ascontiguousarray(tri[:, [3, 4, 5, 6]].astype(np.int32))
+    lr.lr_set_triangles(abc.ctypes.data, nb.ctypes.data, len(tri))
+    tri_id = tri.astype(np.int32).copy()
+    tri_id[:, 6] = np.arange(len(tri))
+    tri_id = np.ascontiguousarray(tri_id)
+    locate = oracle.lib.orc_locate
+    st = ctypes.c_int()
+    xs = np.unique(P[:, 0])
+    ys = np.unique(P[:, 1])
+    rng = np.random.default_rng(9)
+    budget = 1 << 24
+    bad = []
+    n = 0
+    for _ in range(300):
+        i0, i1 = sorted(rng.integers(0, len(xs), 2))
+        j0, j1 = sorted(rng.integers(0, len(ys), 2))
+        if rng.random() < 0.3:
+            i1 = i0  # zero width
+        xlo, xhi, ylo, yhi = float(xs[i0]), float(xs[i1]), float(ys[j0]), float(ys[j1])
+        start, steps = ctypes.c_int(), ctypes.c_int()
+        kind = lr.lr_locate_region(xlo, xhi, ylo, yhi, budget, ctypes.byref(start),
+                                   ctypes.byref(steps))
+        for qx in (xlo, 0.5 * (xlo + xhi), xhi):
+            for qy in (ylo, 0.5 * (ylo + yhi), yhi):
+                want = (locate(tri_id, pos, 0, qx, qy, budget, ctypes.byref(st)), st.value)
+                if kind == KIND_FOUND:
+                    got = (start.value, ORC_OK)
+                elif kind == KIND_MISS:
+                    got = (-1, ORC_MISS)
+                else:
+                    got = (locate(tri_id, pos, start.value, qx, qy, budget - steps.value,
+                                  ctypes.byref(st)), st.value)
+                n += 1
+                if got != want:
+                    bad.append((xlo, xhi, ylo, yhi, qx, qy, kind, got, want))
+    assert n > 2000 and not bad, bad[:3]
