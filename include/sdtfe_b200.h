@@ -131,6 +131,15 @@ dtfe_status_t dtfe_mesh_hull(dtfe_mesh_t mesh, int axis, int *tri /* 8*n_tri or 
 /* Map into a host array (accumulated: map[p] += value, as the reference does). */
 dtfe_status_t dtfe_map(dtfe_mesh_t mesh, const dtfe_map_params_t *p, double *map,
                        dtfe_map_stats_t *stats);
+/* dtfe_map, plus every ray's outcome in host arrays of grid_dim^2 * n_samples
+ * entries, ray (row*G + col)*n_samples + sample: its integral (0 unless
+ * DTFE_RAY_OK), its tet crossings (0 unless DTFE_RAY_OK) and its
+ * dtfe_ray_status_t.  For parity checks of whole maps; the reference's
+ * shoot_3d_ray returns the same two numbers per sample (src/dtfe.c:247-374,
+ * 625-640). */
+dtfe_status_t dtfe_map_rays(dtfe_mesh_t mesh, const dtfe_map_params_t *p, double *map,
+                            double *ray_rho, int *ray_crossed, int *ray_status,
+                            dtfe_map_stats_t *stats);
 /* Map into device memory, asynchronous on `stream` (accumulated as above). */
 dtfe_status_t dtfe_map_device(dtfe_mesh_t mesh, const dtfe_map_params_t *p, double *d_map,
                               void *stream);
@@ -175,13 +184,18 @@ void dtfe_set_seed(uint64_t seed);
  * forbid allocation after start-up).  Inputs and output are device pointers
  * in the reference layouts: d_particle_data (n*4 doubles, column 3 ignored),
  * d_tetra_data (nt*8 ints); d_rho receives n densities, bit-identical to
- * dtfe_mesh_density.  Temporaries live in one static 48 MiB device array held
- * by every GPU that loads the library; sizes that do not fit (about 1.9M
- * tets) are rejected with DTFE_ERR_UNSUPPORTED.  The first call on a device
- * looks up that array's address (cudaGetSymbolAddress): make it before any
- * stream capture.  All calls share the array, so calls that overlap on the
- * GPU (other streams, other host threads) race; the call returns after its
- * work on `stream` (NULL: the default stream) has finished. */
+ * dtfe_mesh_density.  Temporaries live in one static 48 MiB device array;
+ * sizes that do not fit (about 1.9M tets) are rejected with
+ * DTFE_ERR_UNSUPPORTED.  The first call on each device sets the array up
+ * (cudaGetSymbolAddress, with that device current); with CUDA's lazy module
+ * loading that is also when the 48 MiB are reserved on the device, which
+ * then holds them until the process exits.  So make one call per device at
+ * start-up - a call with n_particles == 0 does the set-up alone - before a
+ * memory pool takes the device's memory and before any stream capture.  All
+ * calls share the array, so calls that overlap on the GPU (other streams,
+ * other host threads) race.  The call blocks: it reads a validation flag
+ * back mid-call and returns after its work on `stream` (NULL: the default
+ * stream), which it orders after the stream's earlier work, has finished. */
 dtfe_status_t dtfe_density_noalloc(const double *d_particle_data, int n_particles,
                                    const int *d_tetra_data, int n_tetra, float p_mass,
                                    double *d_rho, void *stream);

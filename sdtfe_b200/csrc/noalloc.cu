@@ -20,9 +20,14 @@
 // -fmad=false for the same reason as mesh.cu.
 //
 // Host code never touches g_density_scratch directly: its name is a host-side
-// stand-in, not a device address.  The first call on each device looks up the
-// array's device address with cudaGetSymbolAddress (with that device current)
-// and caches it; make that first call before any stream capture.
+// stand-in, not a device address.  The first call on each device sets the
+// array up: it looks up the array's device address with cudaGetSymbolAddress
+// (with that device current) and caches it.  With CUDA's lazy module loading
+// that first call is also when the 48 MiB are reserved on the device, so a
+// caller makes one call per device at start-up (n_particles == 0 does only the
+// set-up), before its memory pool takes the device's memory and before any
+// stream capture.  Each call waits on its stream twice (for the validation
+// flag, and for its own work before it returns): it blocks the calling thread.
 #include <cub/device/device_scan.cuh>
 
 #include <cstring>
@@ -127,27 +132,33 @@ extern "C" dtfe_status_t dtfe_density_noalloc(const double* d_particle_data, int
                                               const int* d_tetra_data, int n_tetra, float p_mass,
                                               double* d_rho, void* stream) {
   if (n_particles < 0 || n_tetra < 0) return set_error(DTFE_ERR_INVALID, "negative size");
-  if (n_particles == 0) return DTFE_OK;
+  unsigned char* base = nullptr;
+  if (n_particles == 0) return scratch_base(&base);  // set-up only (the start-up call)
   if (!d_particle_data || !d_rho || (n_tetra > 0 && !d_tetra_data))
     return set_error(DTFE_ERR_INVALID, "NULL device pointer");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int n = n_particles, nt = n_tetra;
-  // carve the scratch: error flag | vol | cnt (n+1) | off (n+1) | idx (4 nt) | scan temp
-  size_t scan_bytes = 0;
-  SDTFE_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int*)nullptr, (int*)nullptr,
-                                           n + 1, s));
+  // carve the scratch: error flag | vol | cnt (n+1) | off (n+1) | idx (4 nt) | scan temp;
+  // the fixed part is checked first, in size_t, so that n + 1 below is an int
   const size_t o_vol = 256;
   const size_t o_cnt = align256(o_vol + sizeof(double) * (size_t)nt);
   const size_t o_off = align256(o_cnt + sizeof(int) * ((size_t)n + 1));
   const size_t o_idx = align256(o_off + sizeof(int) * ((size_t)n + 1));
   const size_t o_tmp = align256(o_idx + sizeof(int) * 4 * (size_t)nt);
+  if (o_tmp > kNoAllocScratchBytes)
+    return set_error(DTFE_ERR_UNSUPPORTED,
+                     "dtfe_density_noalloc: %d particles and %d tets need over %zu bytes of "
+                     "scratch; the static scratch holds %zu (about 1.9M tets)",
+                     n, nt, o_tmp, kNoAllocScratchBytes);
+  size_t scan_bytes = 0;
+  SDTFE_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const int*)nullptr, (int*)nullptr,
+                                           n + 1, s));
   const size_t need = align256(o_tmp + scan_bytes);
   if (need > kNoAllocScratchBytes)
     return set_error(DTFE_ERR_UNSUPPORTED,
                      "dtfe_density_noalloc: %d particles and %d tets need %zu bytes of scratch; "
                      "the static scratch holds %zu (about 1.9M tets)",
                      n, nt, need, kNoAllocScratchBytes);
-  unsigned char* base = nullptr;
   SDTFE_TRY(scratch_base(&base));
   int* err = reinterpret_cast<int*>(base);
   double* vol = reinterpret_cast<double*>(base + o_vol);

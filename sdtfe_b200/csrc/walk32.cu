@@ -809,7 +809,9 @@ __device__ __forceinline__ void tile_rect(const MapArgs32& a, int tile, double* 
 }
 
 // A tile's shared point location (locate_region), packed for the map kernel:
-// (kind | steps << 2, start triangle).
+// (kind | steps << 2 as unsigned bits, start triangle).  steps <= loc_budget
+// = 4 n_tri + 64 < 2^29 + 64 (map_args32 caps n_tri below 2^27), so the
+// packed value fits in 32 unsigned bits; it is unpacked with unsigned shifts.
 __device__ __forceinline__ int2 tile_location(const MapArgs32& a, int tile) {
   int kind = kLocMiss, start = -1, steps = 0;
   if (a.n_tri > 0) {
@@ -817,7 +819,7 @@ __device__ __forceinline__ int2 tile_location(const MapArgs32& a, int tile) {
     tile_rect(a, tile, &xlo, &xhi, &ylo, &yhi);
     kind = locate_region(a.tri, xlo, xhi, ylo, yhi, a.loc_budget, &start, &steps);
   }
-  return make_int2(kind | (steps << 2), start);
+  return make_int2((int)((unsigned)kind | ((unsigned)steps << 2)), start);
 }
 
 // One tile of one map: TW x TH pixels x S samples on BLOCK threads, one ray
@@ -849,13 +851,14 @@ __device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
       const uint64_t rid = (uint64_t)p * (uint64_t)a.S + (uint64_t)s;
       int ft = -1, ft_tri = -1;
       const int2 l = __ldg(loc);
-      const int lk = l.x & 3;
+      const int lk = (int)((unsigned)l.x & 3u);
       if (lk == kLocFound) {
         ft = __ldg(&a.tri[l.y].nb.w);
         ft_tri = l.y;
         status = kRayOk;
       } else if (lk == kLocResume) {
-        ft = locate64(a.tri, l.y, xt, yt, a.loc_budget - (l.x >> 2), &status, &ft_tri);
+        ft = locate64(a.tri, l.y, xt, yt, a.loc_budget - (int)((unsigned)l.x >> 2), &status,
+                      &ft_tri);
       }  // else every ray of the tile leaves the hull (or there is none): a miss
       if (ft >= 0)
         status = walk32(a.rec, a.C, ft, ft_tri, xt, yt, rid, lut, &v, &crossed, &fb, nullptr, 0);
@@ -1112,7 +1115,7 @@ dtfe_status_t map_args32(Mesh& m, const MapGeom& g, int vi, double* d_map,
   a.scale = g.scale;
   a.soff = g.soff;
   a.C = mix_conf(m, g.axis, g.offz, g.lz, g.dist, g.seed, g.max_visits);
-  // the location walk's budget; tile_location packs its steps as steps << 2
+  // the location walk's budget; tile_location packs its steps as unsigned steps << 2
   if (A.n_tri >= (1 << 27))
     return set_error(DTFE_ERR_UNSUPPORTED, "mixed maps over %d hull triangles (at most 2^27 - 1)",
                      A.n_tri);

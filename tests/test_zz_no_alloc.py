@@ -67,3 +67,36 @@ def test_noalloc_rejects_sizes_beyond_the_static_scratch():
     st = f(d.data_ptr(), 1, d.data_ptr(), 50_000_000, 1.0, d.data_ptr(), None)
     assert st == 5  # DTFE_ERR_UNSUPPORTED
     assert b"scratch" in L.dtfe_last_error()
+
+
+def test_noalloc_orders_its_work_after_the_callers_stream(golden):
+    """Inputs uploaded and the output filled on a caller's own stream, behind
+    a slow kernel and with no host synchronisation: the call must run after
+    that work, on that stream, and still return the allocating entry's
+    densities."""
+    import torch
+
+    import sdtfe_b200 as sd
+
+    L, f = _noalloc()
+    a = golden_set(golden, "clustered")
+    with sd.Mesh(a["pos4"], a["tetra"], 1.0) as ma:
+        want = ma.density()
+    assert f(None, 0, None, 0, 0.0, None, None) == 0  # the start-up (set-up only) call
+    h_pos = torch.from_numpy(np.ascontiguousarray(a["pos4"])).pin_memory()
+    h_tet = torch.from_numpy(np.ascontiguousarray(a["tetra"])).pin_memory()
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        d_pos = torch.empty(h_pos.shape, dtype=torch.float64, device="cuda")
+        d_tet = torch.empty(h_tet.shape, dtype=torch.int32, device="cuda")
+        d_rho = torch.empty(len(want), dtype=torch.float64, device="cuda")
+        torch.cuda._sleep(50_000_000)  # the uploads below land well after the call is made
+        d_pos.copy_(h_pos, non_blocking=True)
+        d_tet.copy_(h_tet, non_blocking=True)
+        d_rho.fill_(-7.0)
+        st = f(d_pos.data_ptr(), len(want), d_tet.data_ptr(), len(a["tetra"]), 1.0,
+               d_rho.data_ptr(), side.cuda_stream)
+        assert st == 0, L.dtfe_last_error()
+        got = d_rho.cpu().numpy()
+    assert np.array_equal(got, want)
