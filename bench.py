@@ -88,9 +88,22 @@ def parse():
     return ap.parse_args()
 
 
-def workload(name):
-    from sdtfe_b200 import workloads as W
+def workloads_module():
+    """sdtfe_b200/workloads.py (pure numpy), loaded by path so that the
+    reference arm never imports the sdtfe_b200 package."""
+    import importlib.util
 
+    if "sdtfe_workloads" not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            "sdtfe_workloads", os.path.join(ROOT, "sdtfe_b200", "workloads.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["sdtfe_workloads"] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules["sdtfe_workloads"]
+
+
+def workload(name):
+    W = workloads_module()
     if name == "uniform":
         pos4, spec = W.uniform_box()
         desc = "uniform_32k_256x4"
@@ -198,13 +211,15 @@ class ClockSampler:
 # the reference's CPU implementation
 # ---------------------------------------------------------------------------
 class RefCPU:
-    """The reference's compute_density (its own C, oracle/_ref/libdtfe_ref.so)."""
+    """The reference's compute_density (its own C, oracle/_ref/libdtfe_ref.so),
+    its OpenMP team set to every core this process may run on; `cores` is the
+    team size the reference's OpenMP runtime reports."""
 
     def __init__(self):
         from oracle.oracle import Reference
 
-        self.R = Reference()
-        self.cores = os.cpu_count()
+        self.R = Reference(stock_only=True)
+        self.cores = self.R.set_threads(len(os.sched_getaffinity(0)))
 
     def _quiet(self, fn):
         # the reference prints one stderr line per failed ray; send them to /dev/null
@@ -233,7 +248,6 @@ class RefCPU:
     def calibrate(self, pos4, tetra, spec, seconds):
         """Precompute time (a 4 x 4 window: one tile, negligible walk) and a
         window side whose walk takes about `seconds`."""
-        os.environ.setdefault("OMP_NUM_THREADS", str(self.cores))
         self.t_pre = min(self.window_run(pos4, tetra, spec, 4) for _ in range(2))
         gw = 64
         t = self.window_run(pos4, tetra, spec, gw)
@@ -255,14 +269,29 @@ class RefCPU:
         return spec.rays / full, sample
 
 
+def workload_config(desc, n_particles, n_tets, spec, world):
+    """The `config` object of both arms' lines (identical for the same run)."""
+    return {"workload": desc, "particles": int(n_particles), "tets": int(n_tets),
+            "grid_dim": spec.grid_dim, "samples_per_pixel": spec.n_samples,
+            "rays_per_map": spec.rays, "parallelism": f"replicas x{world}",
+            "l2": f"tet records {n_tets * 320 / 1e6:.0f} MB (mixed walk, 320 B per tet) "
+                  f"{'>' if n_tets * 320 > 126e6 else '<'} the 126 MB L2; the GPU arm flushes "
+                  "L2 between steps (256 MiB write)"}
+
+
 def run_reference(args):
+    """The reference's own CPU code only: the sdtfe_b200 package is not
+    imported in this process (Qhull through SciPy, the reference's tetra_data
+    layout restated in numpy by oracle.oracle.delaunay_tetra)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import sdtfe_b200 as sd
+    from oracle.oracle import delaunay_tetra
 
     desc, pos4, spec = workload(args.workload)
-    tetra = sd.triangulate(pos4)
+    t = time.perf_counter()
+    tetra = delaunay_tetra(pos4)
+    t_qhull = time.perf_counter() - t
     ref = RefCPU()
     ref.calibrate(pos4, tetra, spec, args.cpu_seconds / 3)
     for _ in range(args.warmup):
@@ -280,9 +309,8 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": desc, "particles": len(pos4), "tets": len(tetra),
-                   "grid_dim": spec.grid_dim, "samples_per_pixel": spec.n_samples,
-                   "rays_per_map": spec.rays},
+        "config": workload_config(desc, len(pos4), len(tetra), spec, args.gpus),
+        "qhull_host_s": round(t_qhull, 2),
         "cpu_baseline": {"value": value, "unit": "rays/s", "cores": ref.cores,
                          "kind": "reference", "sample": samples[-1]},
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0,
@@ -727,12 +755,9 @@ def run_ours(args, pre=None):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+guarded-f64" if args.precision == "mixed" else "f64",
             "data": "synthetic (seeded)",
-            "config": {"workload": desc, "particles": len(pos4), "tets": len(tetra),
-                       "grid_dim": G, "samples_per_pixel": S, "rays_per_map": spec.rays,
-                       "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "flushed between steps (256 MiB write); tet records "
-                             f"{len(tetra) * bpv / 1e6:.0f} MB > L2",
-                       "qhull_host_s": round(t_qhull, 2)},
+            "config": workload_config(desc, len(pos4), len(tetra), spec, world),
+            "precision": args.precision,
+            "qhull_host_s": round(t_qhull, 2),
             "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
                            "p99": float(np.percentile(step_ms, 99)),
                            "max": float(step_ms.max())},

@@ -179,8 +179,10 @@ class Reference:
     """The reference's C code.  ``stock`` is the unmodified build; ``harness``
     is the explicit-offset build with the visit hook interposed."""
 
-    def __init__(self):
-        for f in ("libdtfe_ref.so", "libdtfe_refh.so", "libdtfe_refhook.so"):
+    def __init__(self, stock_only=False):
+        libs = ("libdtfe_ref.so",) if stock_only else ("libdtfe_ref.so", "libdtfe_refh.so",
+                                                       "libdtfe_refhook.so")
+        for f in libs:
             if not os.path.exists(os.path.join(REF_DIR, f)):
                 raise FileNotFoundError(f"oracle/_ref/{f} missing: run `make -C oracle ref`")
         self.libc = ctypes.CDLL(None)
@@ -189,6 +191,11 @@ class Reference:
         self._bind(S)
         S.compute_density.argtypes = [_f64, _i, _i32, _i, _i, _d, _d, _f64, ctypes.c_float, _d, _d,
                                       _d, _i, _d]
+        # the stock build's OpenMP runtime (libgomp, a dependency of the library)
+        S.omp_set_num_threads.argtypes = [_i]
+        S.omp_get_max_threads.restype = _i
+        if stock_only:
+            return
         S.compute_3d_density.argtypes = [_f64, _i, _i32, _i, _i, _d, _f64, ctypes.c_float, _d, _d,
                                          _d, ctypes.c_uint]
         S.interpolate_to_3d_grid.argtypes = [_f64, _i, _i32, _i, _i, _d, _f64, _d, _d, _d,
@@ -319,6 +326,12 @@ class Reference:
         return g.reshape(G, G, G)
 
     # -- the stock entry points (libc rand()) --------------------------------
+    def set_threads(self, n):
+        """Sets the OpenMP team size of the stock build's parallel regions and
+        returns the size its runtime reports (omp_get_max_threads)."""
+        self.stock.omp_set_num_threads(int(n))
+        return int(self.stock.omp_get_max_threads())
+
     def compute_density(self, pos4, tetra, G, box_len, box_len_z, rho, p_mass, center, S,
                         delta_sample):
         self.stock.compute_density(pos4, len(pos4), tetra, len(tetra), G, box_len, box_len_z, rho,
