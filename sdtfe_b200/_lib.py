@@ -147,6 +147,8 @@ def lib() -> ctypes.CDLL:
     L.dtfe_mesh_adjacency.argtypes = [_vp, _i32]
     L.dtfe_mesh_hull.argtypes = [_vp, _i, _vp, ctypes.POINTER(_i)]
     L.dtfe_map.argtypes = [_vp, ctypes.POINTER(MapParams), _f64, ctypes.POINTER(MapStats)]
+    L.dtfe_map_rays.argtypes = [_vp, ctypes.POINTER(MapParams), _f64, _f64, _i32, _i32,
+                                ctypes.POINTER(MapStats)]
     L.dtfe_map_device.argtypes = [_vp, ctypes.POINTER(MapParams), _vp, _vp]
     L.dtfe_mesh_last_stats.argtypes = [_vp, ctypes.POINTER(MapStats)]
     L.dtfe_trace.argtypes = [_vp, ctypes.POINTER(MapParams), _i, _f64, _f64, _d, _d, _d, _f64,
@@ -295,12 +297,22 @@ class Mesh:
         _check(lib().dtfe_mesh_hull(self.h, axis, tri.ctypes.data_as(_vp), ctypes.byref(n)))
         return tri[:n.value]
 
-    def map(self, params: MapParams, out: np.ndarray | None = None):
+    def map(self, params: MapParams, out: np.ndarray | None = None, per_ray: bool = False):
+        """(map, MapStats); with per_ray, (map, stats, ray integrals, ray
+        crossings, ray statuses), ray (row*G + col)*n_samples + sample."""
         G = params.grid_dim
         m = np.zeros((G, G), np.float64) if out is None else out
         st = MapStats()
-        _check(lib().dtfe_map(self.h, ctypes.byref(params), m.reshape(-1), ctypes.byref(st)))
-        return m, st
+        if not per_ray:
+            _check(lib().dtfe_map(self.h, ctypes.byref(params), m.reshape(-1), ctypes.byref(st)))
+            return m, st
+        n = G * G * params.n_samples
+        rr = np.zeros(n, np.float64)
+        rc = np.zeros(n, np.int32)
+        rs = np.zeros(n, np.int32)
+        _check(lib().dtfe_map_rays(self.h, ctypes.byref(params), m.reshape(-1), rr, rc, rs,
+                                   ctypes.byref(st)))
+        return m, st, rr, rc, rs
 
     def map_device(self, params: MapParams, d_map_ptr: int, stream_ptr: int = 0):
         _check(lib().dtfe_map_device(self.h, ctypes.byref(params), _vp(d_map_ptr),

@@ -346,6 +346,51 @@ dtfe_status_t dtfe_map(dtfe_mesh_t h, const dtfe_map_params_t* p, double* map,
   return st;
 }
 
+dtfe_status_t dtfe_map_rays(dtfe_mesh_t h, const dtfe_map_params_t* p, double* map,
+                            double* ray_rho, int* ray_crossed, int* ray_status,
+                            dtfe_map_stats_t* stats) {
+  if (!h || !map || !ray_rho || !ray_crossed || !ray_status)
+    return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  SDTFE_TRY(check_params(m, p));
+  const size_t n_rays = (size_t)p->grid_dim * p->grid_dim * p->n_samples;
+  if (n_rays > (size_t)1 << 31)
+    return set_error(DTFE_ERR_UNSUPPORTED, "dtfe_map_rays: %zu rays (at most 2^31)", n_rays);
+  SDTFE_TRY(prepare_axis(m, p->axis, p->precision));
+  cudaStream_t s = m.stream;
+  const size_t bytes = sizeof(double) * (size_t)p->grid_dim * p->grid_dim;
+  void* d[4] = {nullptr, nullptr, nullptr, nullptr};  // map, rho, crossed, status
+  const size_t sz[4] = {bytes, sizeof(double) * n_rays, sizeof(int) * n_rays, sizeof(int) * n_rays};
+  void* host[4] = {map, ray_rho, ray_crossed, ray_status};
+  dtfe_status_t st = DTFE_OK;
+  for (int k = 0; k < 4 && st == DTFE_OK; ++k) {
+    const cudaError_t e = cudaMallocAsync(&d[k], sz[k], s);
+    if (e != cudaSuccess)
+      st = set_error(e == cudaErrorMemoryAllocation ? DTFE_ERR_NOMEM : DTFE_ERR_CUDA,
+                     "map_rays: %s", cudaGetErrorString(e));
+  }
+  if (st == DTFE_OK) {
+    const cudaError_t e = cudaMemcpyAsync(d[0], map, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "map_rays: %s", cudaGetErrorString(e));
+  }
+  if (st == DTFE_OK)
+    st = launch_map(m, p, static_cast<double*>(d[0]), s, static_cast<double*>(d[1]),
+                    static_cast<int*>(d[2]), static_cast<int*>(d[3]));
+  for (int k = 0; k < 4 && st == DTFE_OK; ++k) {
+    const cudaError_t e = cudaMemcpyAsync(host[k], d[k], sz[k], cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "map_rays: %s", cudaGetErrorString(e));
+  }
+  if (st == DTFE_OK) {
+    const cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "map_rays: %s", cudaGetErrorString(e));
+  }
+  for (int k = 0; k < 4; ++k)
+    if (d[k]) cudaFreeAsync(d[k], s);
+  if (st == DTFE_OK && stats) st = read_stats(m, stats);
+  return st;
+}
+
 dtfe_status_t dtfe_trace(dtfe_mesh_t h, const dtfe_map_params_t* p, int n_rays, const double* x,
                          const double* y, double z0, double lz, double delta_xy, double* rho,
                          int* crossed, int* status, int* visits, int max_record) {
