@@ -75,11 +75,12 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--sections", default="batch,serving",
+    ap.add_argument("--sections", default="batch,serving,large_field",
                     help="extra sections on one GPU: batch (64 cutouts in one persistent launch), "
                          "serving (request stream with continuous batching); 'none' to skip")
     ap.add_argument("--serve-handles", type=int, default=256)
-    ap.add_argument("--serve-distinct", type=int, default=32)
+    ap.add_argument("--serve-distinct", type=int, default=256,
+                    help="distinct cutout triangulations behind the handles (default: one per handle)")
     ap.add_argument("--serve-requests", type=int, default=200)
     ap.add_argument("--serve-load", type=float, default=0.7,
                     help="Poisson arrival rate as a fraction of the measured mixed capacity")
@@ -127,6 +128,8 @@ def _qhull_task(task):
         pos4 = workload(key)[1]
     elif kind == "cutout":
         pos4 = W.halo_cutout(n, seed)
+    elif kind == "large":
+        pos4 = W.perturbed_lattice()
     else:  # "clustered": the clustered-box recipe at n particles
         pos4 = W.clustered_box(n=n, seed=seed)[0]
     t = time.perf_counter()
@@ -134,21 +137,44 @@ def _qhull_task(task):
     return kind, key, pos4, tetra, time.perf_counter() - t
 
 
-def triangulate_all(tasks):
-    """Runs the Qhull tasks in a spawn process pool, largest first.  Called
-    before the first CUDA call of the process."""
-    import multiprocessing as mp
+class QhullPool:
+    """Host Qhull for every workload of the run in a spawn process pool, the
+    main workload first, then the largest: sections that need a
+    triangulation wait for it (get), so GPU work on the ones already done
+    overlaps the rest."""
 
-    procs = max(1, min(len(tasks), len(os.sched_getaffinity(0)), 32))
-    order = sorted(tasks, key=lambda t: -t[2])
-    out, cpu_s = {}, 0.0
-    t = time.perf_counter()
-    with mp.get_context("spawn").Pool(procs) as pool:
-        for kind, key, pos4, tetra, dt in pool.imap_unordered(_qhull_task, order, chunksize=1):
-            out[(kind, key)] = (pos4, tetra, dt)
-            cpu_s += dt
-    return out, {"procs": procs, "wall_s": round(time.perf_counter() - t, 1),
-                 "cpu_s": round(cpu_s, 1)}
+    def __init__(self, tasks):
+        import multiprocessing as mp
+
+        self.procs = max(1, min(len(tasks), len(os.sched_getaffinity(0)), 32))
+        order = tasks[:1] + sorted(tasks[1:], key=lambda t: -t[2])
+        self.t0 = time.perf_counter()
+        self.pool = mp.get_context("spawn").Pool(self.procs)
+        self.pending = {(t[0], t[1]): self.pool.apply_async(_qhull_task, (t,)) for t in order}
+        self.done, self.cpu_s, self.wall_s = {}, 0.0, None
+
+    def get(self, kind, key):
+        if (kind, key) not in self.done:
+            _, _, pos4, tetra, dt = self.pending.pop((kind, key)).get()
+            self.done[(kind, key)] = (pos4, tetra, dt)
+            self.cpu_s += dt
+        return self.done[(kind, key)]
+
+    def drop(self, kind, key):
+        self.done.pop((kind, key), None)
+
+    def wait_all(self):
+        """Every triangulation finished and the pool closed (host cores idle)."""
+        for kind, key in list(self.pending):
+            self.get(kind, key)
+        if self.wall_s is None:
+            self.wall_s = time.perf_counter() - self.t0
+            self.pool.close()
+            self.pool.join()
+
+    def info(self):
+        return {"procs": self.procs, "wall_s": round(self.wall_s or 0.0, 1),
+                "cpu_s": round(self.cpu_s, 1)}
 
 
 # ---------------------------------------------------------------------------
@@ -322,16 +348,49 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def read_ncu_traffic(kernel, n_tets):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/traffic.json), scaled from the captured mesh to this one by the
-    tet count: the walk reads each tet record from DRAM about once per map."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+def read_profile(kernel):
+    """The committed ncu figures of `kernel` (profiles/roofline.json): the
+    captured workload's tets and tet visits, and per launch its warp
+    instructions, threads per warp instruction, DRAM bytes and cache hit
+    rates."""
     try:
-        d = json.load(open(path))[kernel]
-        return d["dram_bytes"] / d["tets"] * n_tets
-    except (OSError, KeyError, ValueError, ZeroDivisionError):
+        return json.load(open(os.path.join(ROOT, "profiles", "roofline.json")))[kernel]
+    except (OSError, KeyError, ValueError):
         return None
+
+
+def roofline(kernel, visits, n_tets, bytes_per_visit, kern_ms, sm_mhz, n_sm, hbm_peak, hbm_note):
+    """The walk kernel against its bound, instruction issue: each SM issues at
+    most one warp instruction per scheduler (4) per cycle, so the peak is
+    SMs x 4 x the SM clock sampled during the timed region.  achieved = this
+    launch's tet visits x the warp instructions per visit that ncu counted on
+    the profiled workload, over the event-timed duration.  DRAM traffic is the
+    profile's bytes per tet (each tet's records are read from DRAM about once
+    per map), scaled to this mesh; the algorithmic bytes (96 B per mixed
+    visit) are mostly served from L1/L2, and are reported beside it."""
+    t = kern_ms / 1e3
+    alg_gbs = visits * bytes_per_visit / t / 1e9
+    prof = read_profile(kernel)
+    if not prof:  # no committed profile: the algorithmic-bytes figure alone
+        return {"bound": "hbm", "achieved": alg_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": alg_gbs / hbm_peak, "traffic": None, "kernel": kernel,
+                "note": f"peak {hbm_note}; no ncu profile committed for {kernel}"}
+    wipv = prof["warp_inst"] / prof["visits"]
+    achieved = visits * wipv / t
+    peak = n_sm * 4 * sm_mhz * 1e6
+    traffic = prof["dram_bytes"] / prof["tets"] * n_tets
+    return {"bound": "issue", "achieved": achieved / 1e9, "peak": peak / 1e9,
+            "unit": "G warp-instructions/s", "frac": achieved / peak, "traffic": traffic,
+            "kernel": kernel, "warp_inst_per_visit": wipv,
+            "threads_per_warp_inst": prof.get("threads_per_warp_inst"),
+            "issue_active_pct_profiled": prof.get("issue_active_pct"),
+            "dram_gbs": traffic / t / 1e9, "dram_frac": traffic / t / 1e9 / hbm_peak,
+            "hbm_peak_gbs": hbm_peak, "hbm_peak_note": hbm_note,
+            "l1_hit_pct": prof.get("l1_hit_pct"), "l2_hit_pct": prof.get("l2_hit_pct"),
+            "algorithmic_gbs": alg_gbs, "bytes_per_visit": bytes_per_visit,
+            "sm_mhz": sm_mhz, "sms": n_sm, "profile": prof.get("source"),
+            "note": "peak = SMs x 4 schedulers x sampled SM clock; warp instructions per visit "
+                    "and DRAM bytes per tet from the committed ncu capture"}
 
 
 def slowest_rank_ms(total_ms, dist, device):
@@ -352,8 +411,8 @@ def replica_rays_per_s(rays_per_map, steps, world, total_ms):
 
 
 def plan_sections(args):
-    """Qhull for the main workload and the sections, in a process pool, before
-    any CUDA call (sections run at N=1 only)."""
+    """Starts host Qhull for the main workload and the sections (N=1 only) in
+    a spawn process pool; returns (pool, sections)."""
     from sdtfe_b200 import workloads as W
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -365,10 +424,22 @@ def plan_sections(args):
     if "batch" in sections:
         tasks += [("cutout", i, n, seed) for i, (n, seed, _) in enumerate(W.cutout_specs())]
     if "serving" in sections:
-        tasks += [("clustered", i, n, seed)
-                  for i, (n, seed) in enumerate(W.serving_cutouts(args.serve_distinct))]
-    tri, qinfo = triangulate_all(tasks)
-    return tri, qinfo, sections
+        tasks += [("clustered", i, n, seed) for i, (n, seed) in enumerate(serving_cutouts(args))]
+    if "large_field" in sections:
+        tasks += [("large", 0, 9_201_254, 5)]
+    return QhullPool(tasks), sections
+
+
+def serving_cutouts(args):
+    """(particle count, seed) of the serving stream's resident cutouts: the
+    stream's own counts (log-uniform in [1e4, 2e6]) and the clustered-box
+    recipe, one distinct cutout per handle unless --serve-distinct is
+    smaller (then handle h holds cutout h % distinct)."""
+    from sdtfe_b200 import workloads as W
+
+    ns, _ = W.serving_stream(n_cutouts=args.serve_handles, n_requests=args.serve_requests)
+    k = min(args.serve_distinct, args.serve_handles)
+    return [(int(ns[i]), 4 * 1000 + i) for i in range(k)]
 
 
 def timed_launches(torch, stream, flush, fn, steps):
@@ -400,7 +471,7 @@ def section_batch(args, sd, torch, dev, stream, flush, tri):
     specs = W.cutout_specs()
     meshes, p32, p64, d32, d64 = [], [], [], [], []
     for i, (n, seed, sp) in enumerate(specs):
-        pos4, tetra, _ = tri[("cutout", i)]
+        pos4, tetra, _ = tri.get("cutout", i)
         meshes.append(sd.Mesh(pos4, tetra, 1.0))
         kw = dict(seed=5000 + i)
         p32.append(sd.map_params(sp.grid_dim, sp.box_len, sp.box_len_z, sp.center, sp.n_samples,
@@ -533,17 +604,21 @@ def section_serving(args, sd, torch, tri):
     at a fraction of the mixed capacity, mixed vs FP64."""
     from sdtfe_b200 import workloads as W
 
-    cut = W.serving_cutouts(args.serve_distinct)
+    cut = serving_cutouts(args)
     meshes = []
     for h in range(args.serve_handles):
-        pos4, tetra, _ = tri[("clustered", h % len(cut))]
-        meshes.append(sd.Mesh(pos4, tetra, 1.0))
+        pos4, tetra, _ = tri.get("clustered", h % len(cut))
+        # no walk records at creation: the serving loop builds what requests need
+        meshes.append(sd.Mesh(pos4, tetra, 1.0, sd.MESH_LAZY))
+    for h in range(len(cut)):
+        tri.drop("clustered", h)  # the meshes keep their own host copies
     _, reqs = W.serving_stream(n_cutouts=args.serve_handles, n_requests=args.serve_requests)
     out = {"workload": f"{args.serve_handles} resident cutouts ({len(cut)} distinct "
-                       "clustered-box triangulations, N log-uniform [1e4, 5e5]); "
+                       "clustered-box triangulations, N log-uniform [1e4, 2e6]); "
                        f"{len(reqs)} requests: random cutout, axis, side in "
                        "{128..2048}, 4-16 samples/pixel",
-           "particles_resident": int(sum(cut[h % len(cut)][0] for h in range(args.serve_handles)))}
+           "particles_resident": int(sum(cut[h % len(cut)][0] for h in range(args.serve_handles))),
+           "tets_resident": int(sum(m.info().n_tetra for m in meshes))}
     with sd.Server(quantum_rays=args.serve_quantum) as srv:
         ids = [srv.add_mesh(m) for m in meshes]
         # warm-up: one small request per cutout touches every handle once
@@ -569,6 +644,74 @@ def section_serving(args, sd, torch, tri):
     return out
 
 
+def section_large_field(args, sd, torch, dev, stream, flush, tri):
+    """The large field: a 192^3 perturbed lattice plus 30% of its count in
+    2,000 r^-2 clusters (float32), one 8192^2 x 4 z-projection and one 512^3
+    grid (supersampling 1, the reference's column walk), mixed against FP64:
+    device time, crossings, max/RMS relative error, projected mass."""
+    pos4, tetra, t_q = tri.get("large", 0)
+    mesh = sd.Mesh(pos4, tetra, 1.0, sd.MESH_LAZY)
+    tri.drop("large", 0)
+    info = mesh.info()
+    sptr = stream.cuda_stream
+    out = {"workload": "192^3 lattice (sigma 0.3 spacing) + 30% in 2000 r^-2 clusters (r 0.01), "
+                       "float32; 8192^2 x 4 map and 512^3 grid (ss 1), mixed vs FP64",
+           "particles": int(len(pos4)), "tets": int(info.n_tetra), "qhull_host_s": round(t_q, 1)}
+    G, S = 8192, 4
+    kw = dict(grid_dim=G, box_len=1.0, box_len_z=1.0, center=(0.5, 0.5, 0.5), n_samples=S,
+              seed=909)
+    d_map = torch.zeros(G * G, dtype=torch.float64, device=dev)
+    res = {}
+    for name, prec, reps in (("mixed", sd.DTFE_MIXED, 2), ("fp64", sd.DTFE_FP64, 1)):
+        p = sd.map_params(**kw, precision=prec)
+
+        def one(p=p):
+            d_map.zero_()
+            mesh.map_device(p, d_map.data_ptr(), sptr)
+        one()  # builds the records, warms up
+        ms = timed_launches(torch, stream, flush, one, reps)
+        st = mesh.last_stats()
+        res[name] = (float(np.median(ms)), st, d_map.cpu().numpy())
+    rays = G * G * S
+    (m32, s32, a32), (m64, s64, a64) = res["mixed"], res["fp64"]
+    e_max, e_rms = max_rel(a32, a64)
+    out["map"] = {"rays": rays, "mixed_ms": m32, "fp64_ms": m64,
+                  "mixed_rays_per_s": rays / (m32 / 1e3), "fp64_rays_per_s": rays / (m64 / 1e3),
+                  "speedup_mixed_over_fp64": m64 / m32, "visits_per_ray": s32.visits / rays,
+                  "visits_equal_fp64": bool(s32.visits == s64.visits),
+                  "status_equal_fp64": list(s32.status) == list(s64.status),
+                  "fp64_fallbacks": s32.fp64_fallbacks,
+                  "max_rel_err": e_max, "rms_rel_err": e_rms,
+                  "mass_rel_diff": float(a32.sum() / G / G / len(pos4) - 1.0),
+                  "hull_triangles": int(info.n_hull_tri[0]) if info.n_hull_tri[0] >= 0 else None}
+    del d_map, res
+    torch.cuda.empty_cache()
+    GG = 512
+    d_grid = torch.zeros(GG ** 3, dtype=torch.float64, device=dev)
+    gres = {}
+    for name, prec in (("mixed", sd.DTFE_MIXED), ("fp64", sd.DTFE_FP64)):
+        def one(prec=prec):
+            d_grid.zero_()
+            mesh.grid_device(GG, 1.0, (0.5, 0.5, 0.5), 1, 77, d_grid.data_ptr(), precision=prec,
+                             stream_ptr=sptr)
+        one()
+        ms = timed_launches(torch, stream, flush, one, 2)
+        gres[name] = (float(np.median(ms)), mesh.last_stats(), d_grid.cpu().numpy())
+    (g32ms, gs32, g32), (g64ms, gs64, g64) = gres["mixed"], gres["fp64"]
+    e_max, e_rms = max_rel(g32, g64)
+    out["grid"] = {"grid_dim": GG, "columns": GG * GG, "mixed_ms": g32ms, "fp64_ms": g64ms,
+                   "speedup_mixed_over_fp64": g64ms / g32ms,
+                   "visits_equal_fp64": bool(gs32.visits == gs64.visits),
+                   "status_equal_fp64": list(gs32.status) == list(gs64.status),
+                   "zero_cells_equal": bool(np.array_equal(g32 == 0, g64 == 0)),
+                   "max_rel_err": e_max, "rms_rel_err": e_rms,
+                   "mass_rel_diff": float(g32.sum() / GG ** 3 / len(pos4) - 1.0)}
+    del d_grid, gres
+    mesh.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args, pre=None):
     import torch
 
@@ -590,14 +733,14 @@ def run_ours(args, pre=None):
 
     desc, pos4, spec = workload(args.workload)
     tri = sections = None
-    if pre is not None:  # host Qhull ran in the process pool before CUDA started
-        tri, qinfo, sections = pre
-        _, tetra, t_qhull = tri[("main", args.workload)]
+    if pre is not None:  # host Qhull runs in the process pool
+        tri, sections = pre
+        _, tetra, t_qhull = tri.get("main", args.workload)
     else:
         t = time.perf_counter()
         tetra = sd.triangulate(pos4)
         t_qhull = time.perf_counter() - t
-        qinfo, sections = None, []
+        sections = []
     prec = sd.DTFE_MIXED if args.precision == "mixed" else sd.DTFE_FP64
     mesh = sd.Mesh(pos4, tetra, 1.0)
     G, S = spec.grid_dim, spec.n_samples
@@ -679,6 +822,23 @@ def run_ours(args, pre=None):
                 "rms_rel_err": float(np.sqrt(np.mean(rel ** 2))) if rel.size else 0.0,
                 "zero_pixels_differ": int(((map64 == 0) != (mixed_map == 0)).sum()),
                 "visits_equal": bool(st64.visits == st.visits)}
+    # device-timed sections run while host Qhull for the others continues;
+    # everything host-timed (e2e, the CPU baseline, serving latency) runs
+    # after the pool has finished, on idle host cores
+    extra = {}
+
+    def run_section(name, fn):
+        if sections and name in sections:
+            try:
+                extra[name] = fn()
+            except Exception as e:  # a section must not cost the headline line
+                extra[name] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.synchronize()
+
+    run_section("batch", lambda: section_batch(args, sd, torch, dev, stream, flush, tri))
+    if tri is not None:
+        tri.wait_all()
+
     # projected mass inside the map footprint (unit box fully covered)
     dxy = spec.box_len / G
     mass_map = float(mixed_map.sum() * dxy * dxy)
@@ -712,17 +872,17 @@ def run_ours(args, pre=None):
     visits = st.visits  # one launch
     bpv = BYTES_PER_VISIT[args.precision]
     kern_ms = float(np.median(step_ms))
-    achieved = visits * bpv / (kern_ms / 1e3) / 1e9
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         pass
-    peak = peaks.get("hbm_gbs")
-    peak_note = "measured" if peak else "fallback"
-    peak = peak or 6650.0
+    hbm = peaks.get("hbm_gbs")
+    hbm_note = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
     kname = "k_map32" if args.precision == "mixed" else "k_map64"
-    traffic = read_ncu_traffic(kname, len(tetra))
+    roof = roofline(kname, visits, len(tetra), bpv, kern_ms, clk.get("sm_mhz") or 1965.0,
+                    torch.cuda.get_device_properties(dev).multi_processor_count, hbm, hbm_note)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -736,17 +896,11 @@ def run_ours(args, pre=None):
             cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
 
-    extra = {}
-    for name, fn in (("batch", lambda: section_batch(args, sd, torch, dev, stream, flush, tri)),
-                     ("serving", lambda: section_serving(args, sd, torch, tri))):
-        if sections and name in sections:
-            try:
-                extra[name] = fn()
-            except Exception as e:  # a section must not cost the headline line
-                extra[name] = {"error": f"{type(e).__name__}: {e}"}
-            torch.cuda.synchronize()
-    if qinfo:
-        extra["qhull_pool"] = qinfo
+    run_section("serving", lambda: section_serving(args, sd, torch, tri))
+    run_section("large_field",
+                lambda: section_large_field(args, sd, torch, dev, stream, flush, tri))
+    if tri is not None:
+        extra["qhull_pool"] = tri.info()
 
     if rank == 0:
         line = {
@@ -772,11 +926,7 @@ def run_ours(args, pre=None):
                     "d2h_bytes_per_step": int(d2h),
                     "ms_per_step": float(np.median(e2e_ms)) if e2e_ms else None,
                     "call": "compute_density (dtfe.h drop-in), pinned host buffers"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": kname, "bytes_per_visit": bpv,
-                         "note": f"peak {peak_note} (STREAM-style copy); achieved counts "
-                                 "algorithmic tet-record bytes, much of it served by L1/L2"},
+            "roofline": roof,
             "cpu_baseline": cpu,
             "autotune": tuned,
             "clocks": clk,

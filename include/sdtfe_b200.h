@@ -104,6 +104,9 @@ typedef struct {
 /* mesh flags */
 #define DTFE_MESH_FIELD 1u       /* column 3 is a field: skip the density step      */
 #define DTFE_MESH_NO_FP64_REC 2u /* keep no FP64 walk records (MIXED maps only)     */
+#define DTFE_MESH_LAZY 4u        /* build no walk records or hull at creation: the
+                                    first map (or the serving loop) builds what it
+                                    needs; for meshes held in bulk                */
 
 const char *dtfe_last_error(void);
 void dtfe_clear_error(void); /* empty the calling thread's last-error message */
@@ -111,7 +114,8 @@ const char *dtfe_status_string(dtfe_status_t s);
 
 /* Upload a mesh and build everything the walks need: densities, gradients, and
  * the z axis' hull and walk records for the default precision (other axes and
- * precisions are built on first use).  Unless DTFE_MESH_FIELD is set, column 3
+ * precisions are built on first use; with DTFE_MESH_LAZY the z axis' are too).
+ * Unless DTFE_MESH_FIELD is set, column 3
  * of particle_data is ignored and replaced on the device by the DTFE density
  * 4*p_mass / (sum of adjacent |V|) (src/triangulate.c:183-225). */
 dtfe_status_t dtfe_mesh_create(const double *particle_data, int n_particles,
@@ -158,6 +162,17 @@ dtfe_status_t dtfe_trace(dtfe_mesh_t mesh, const dtfe_map_params_t *p, int n_ray
  * G^3 doubles, accumulated; grid[(i*G + j)*G + iz], i along x and j along y. */
 dtfe_status_t dtfe_grid(dtfe_mesh_t mesh, int grid_dim, double box_len, const double center[3],
                         unsigned supersampling, uint64_t seed, double *grid);
+/* The same grid with the walk's arithmetic chosen: DTFE_FP64 (dtfe_grid) or
+ * DTFE_MIXED (FP32 walk, guarded FP64: the same tets crossed, each fine node
+ * assigned to the FP64 path's tet, cells within 1e-5 relative of FP64). */
+dtfe_status_t dtfe_grid_ex(dtfe_mesh_t mesh, int grid_dim, double box_len, const double center[3],
+                           unsigned supersampling, uint64_t seed, int precision, double *grid);
+/* Grid into device memory (G^3 doubles, accumulated), asynchronous on
+ * `stream` (NULL: the handle's stream); dtfe_mesh_last_stats gives its
+ * counters and kernel time. */
+dtfe_status_t dtfe_grid_device(dtfe_mesh_t mesh, int grid_dim, double box_len,
+                               const double center[3], unsigned supersampling, uint64_t seed,
+                               int precision, double *d_grid, void *stream);
 
 /* Autotuner for the mixed-precision map kernel: times every variant on a
  * central window of the map p describes (same pixel size and samples, about a
@@ -251,7 +266,9 @@ typedef struct dtfe_server_s *dtfe_server_t;
 #define DTFE_SERVE_FIFO 1  /* each iteration serves the oldest requests first      */
 
 typedef struct {
-  size_t device_budget;    /* bytes for walk records and maps (0: 3/4 of free memory) */
+  size_t device_budget;    /* bytes for walk records and maps (0: the free device
+                              memory less a reserve of 5% (at least 2 GiB), plus the
+                              records of the meshes as they are registered)      */
   int max_active;          /* requests on the GPU at once (0: 64)                     */
   long long quantum_rays;  /* rays per iteration launch under light load (0: 2^20);
                               with a backlog up to 8x this                           */
@@ -304,6 +321,18 @@ typedef int (*dtfe_triangulator_fn)(const double *xyz4, int n, const char *optio
                                     int **simplices, int **neighbors, size_t *n_tetra,
                                     void *user);
 void dtfe_set_triangulator(dtfe_triangulator_fn fn, void *user);
+/* triangulate() keeps its recent results, keyed by the exact input (the
+ * count, the options and every x, y, z), and answers a repeated input with a
+ * copy of the stored rows without running the backend: Qhull is deterministic
+ * for one input order and option set, so the rows are the ones it would
+ * return.  No counterpart in the reference, which triangulates on every call
+ * (python/pydtfe.cpp:54, src/main.c:160).  max_bytes bounds the host memory
+ * held (coordinates and rows; least recently used entries go first); 0
+ * disables the cache and empties it.  The default limit is the
+ * SDTFE_TRI_CACHE_MB environment variable, else 1024 MB. */
+void dtfe_set_triangulation_cache(size_t max_bytes);
+void dtfe_triangulation_cache_stats(unsigned long long *hits, unsigned long long *misses,
+                                    size_t *entries, size_t *bytes);
 /* The layout step of triangulate() (src/triangulate.c:63-175): Qhull cells to
  * tetra_data rows, swapping B and C (and their neighbours) where
  * (AB x AC) . AD > 0.  tetra_out holds nt*8 ints. */

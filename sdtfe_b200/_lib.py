@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libsdtfe_b200.so")
 
 DTFE_FP64, DTFE_MIXED = 0, 1
 AXIS_Z, AXIS_X, AXIS_Y = 0, 1, 2
-MESH_FIELD, MESH_NO_FP64_REC = 1, 2
+MESH_FIELD, MESH_NO_FP64_REC, MESH_LAZY = 1, 2, 4
 RAY_OK, RAY_MISS, RAY_NO_EXIT, RAY_PERTURB_MAX, RAY_BUDGET, RAY_LOC_BUDGET = range(6)
 N_RAY_STATUS = 6
 
@@ -154,6 +154,16 @@ def lib() -> ctypes.CDLL:
     L.dtfe_trace.argtypes = [_vp, ctypes.POINTER(MapParams), _i, _f64, _f64, _d, _d, _d, _f64,
                              _i32, _i32, _vp, _i]
     L.dtfe_grid.argtypes = [_vp, _i, _d, _d * 3, ctypes.c_uint, ctypes.c_uint64, _f64]
+    L.dtfe_grid_ex.argtypes = [_vp, _i, _d, _d * 3, ctypes.c_uint, ctypes.c_uint64, _i, _f64]
+    L.dtfe_grid_device.argtypes = [_vp, _i, _d, _d * 3, ctypes.c_uint, ctypes.c_uint64, _i, _vp,
+                                   _vp]
+    L.dtfe_set_triangulation_cache.argtypes = [ctypes.c_size_t]
+    L.dtfe_set_triangulation_cache.restype = None
+    L.dtfe_triangulation_cache_stats.argtypes = [ctypes.POINTER(ctypes.c_ulonglong),
+                                                 ctypes.POINTER(ctypes.c_ulonglong),
+                                                 ctypes.POINTER(ctypes.c_size_t),
+                                                 ctypes.POINTER(ctypes.c_size_t)]
+    L.dtfe_triangulation_cache_stats.restype = None
     L.dtfe_set_default_precision.argtypes = [_i]
     L.dtfe_set_seed.argtypes = [ctypes.c_uint64]
     L.dtfe_kernel_launches.restype = ctypes.c_ulonglong
@@ -349,11 +359,18 @@ class Mesh:
                                 max_record))
         return rho, crossed, status, visits
 
-    def grid(self, G, box_len, center, ss, seed, out: np.ndarray | None = None) -> np.ndarray:
+    def grid(self, G, box_len, center, ss, seed, out: np.ndarray | None = None,
+             precision: int = DTFE_FP64) -> np.ndarray:
         g = np.zeros((G, G, G), np.float64) if out is None else out
         c = (_d * 3)(*center)
-        _check(lib().dtfe_grid(self.h, G, box_len, c, ss, seed, g.reshape(-1)))
+        _check(lib().dtfe_grid_ex(self.h, G, box_len, c, ss, seed, precision, g.reshape(-1)))
         return g
+
+    def grid_device(self, G, box_len, center, ss, seed, d_grid_ptr: int,
+                    precision: int = DTFE_FP64, stream_ptr: int = 0):
+        c = (_d * 3)(*center)
+        _check(lib().dtfe_grid_device(self.h, G, box_len, c, ss, seed, precision, _vp(d_grid_ptr),
+                                      _vp(stream_ptr) if stream_ptr else None))
 
 
 class Batch:

@@ -155,7 +155,7 @@ dtfe_status_t dtfe_mesh_create(const double* particle_data, int n_particles, con
   dtfe_status_t s = mesh_upload(&m, particle_data, n_particles, tetra_data, n_tetra, p_mass, flags);
   if (s == DTFE_OK && !(flags & DTFE_MESH_FIELD)) s = mesh_density(&m);
   if (s == DTFE_OK) s = mesh_gradients(&m);
-  if (s == DTFE_OK) {
+  if (s == DTFE_OK && !(flags & DTFE_MESH_LAZY)) {
     // the z-axis records and hull for the precision maps use by default
     const int prec = (flags & DTFE_MESH_NO_FP64_REC) ? DTFE_MIXED : dtfe_get_default_precision();
     s = prepare_axis(m, DTFE_AXIS_Z, prec);
@@ -442,31 +442,72 @@ dtfe_status_t dtfe_trace(dtfe_mesh_t h, const dtfe_map_params_t* p, int n_rays, 
   return st;
 }
 
-dtfe_status_t dtfe_grid(dtfe_mesh_t h, int G, double box_len, const double center[3],
-                        unsigned ss, uint64_t seed, double* grid) {
-  if (!h || !center || !grid) return set_error(DTFE_ERR_INVALID, "NULL argument");
+namespace {
+
+dtfe_status_t check_grid(dtfe_mesh_t h, int G, double box_len, const double* center, unsigned ss,
+                         int precision) {
+  if (!h || !center) return set_error(DTFE_ERR_INVALID, "NULL argument");
   if (G < 1 || ss < 1) return set_error(DTFE_ERR_INVALID, "grid_dim and supersampling must be >= 1");
   if (!(box_len > 0)) return set_error(DTFE_ERR_INVALID, "box_len must be > 0");
   if ((double)G * G * G * sizeof(double) > 1e12)
     return set_error(DTFE_ERR_UNSUPPORTED, "grid_dim %d: grid larger than 1 TB", G);
+  if (precision != DTFE_FP64 && precision != DTFE_MIXED)
+    return set_error(DTFE_ERR_INVALID, "precision %d unknown", precision);
+  if (precision == DTFE_FP64 && (h->m.flags & DTFE_MESH_NO_FP64_REC))
+    return set_error(DTFE_ERR_INVALID, "FP64 grid on a mesh built with DTFE_MESH_NO_FP64_REC");
+  return DTFE_OK;
+}
+
+// with h->mu held
+dtfe_status_t launch_grid(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
+                          uint64_t seed, int precision, double* d, cudaStream_t s) {
+  if (!m.has_density) return set_error(DTFE_ERR_INVALID, "mesh has no density");
+  SDTFE_TRY(prepare_axis(m, DTFE_AXIS_Z, precision));
+  if (precision == DTFE_MIXED) SDTFE_TRY(mesh_field64(&m));
+  if (s != m.stream) SDTFE_CUDA(cudaStreamSynchronize(m.stream));  // records are built there
+  const int max_visits = (int)((2LL * m.nt + 64) > 0x7fffffff ? 0x7fffffff : (2LL * m.nt + 64));
+  if (precision == DTFE_MIXED) return launch_grid32(m, G, box_len, center, ss, seed, max_visits, d, s);
+  return launch_grid64(m, G, box_len, center, ss, seed, max_visits, d, s);
+}
+
+}  // namespace
+
+dtfe_status_t dtfe_grid_ex(dtfe_mesh_t h, int G, double box_len, const double center[3],
+                           unsigned ss, uint64_t seed, int precision, double* grid) {
+  SDTFE_TRY(check_grid(h, G, box_len, center, ss, precision));
+  if (!grid) return set_error(DTFE_ERR_INVALID, "NULL argument");
   std::lock_guard<std::mutex> lk(h->mu);
   Mesh& m = h->m;
-  if (!m.has_density) return set_error(DTFE_ERR_INVALID, "mesh has no density");
-  SDTFE_TRY(prepare_axis(m, DTFE_AXIS_Z, DTFE_FP64));
   cudaStream_t s = m.stream;
   const size_t bytes = sizeof(double) * (size_t)G * G * G;
   double* d = nullptr;
   SDTFE_CUDA(cudaMallocAsync(&d, bytes, s));
-  SDTFE_CUDA(cudaMemcpyAsync(d, grid, bytes, cudaMemcpyHostToDevice, s));
-  const int max_visits = (int)((2LL * m.nt + 64) > 0x7fffffff ? 0x7fffffff : (2LL * m.nt + 64));
-  dtfe_status_t st = launch_grid64(m, G, box_len, center, ss, seed, max_visits, d, s);
+  cudaError_t e = cudaMemcpyAsync(d, grid, bytes, cudaMemcpyHostToDevice, s);
+  dtfe_status_t st = e == cudaSuccess ? launch_grid(m, G, box_len, center, ss, seed, precision, d, s)
+                                      : set_error(DTFE_ERR_CUDA, "grid: %s", cudaGetErrorString(e));
   if (st == DTFE_OK) {
-    cudaError_t e = cudaMemcpyAsync(grid, d, bytes, cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(grid, d, bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "grid: %s", cudaGetErrorString(e));
   }
   cudaFreeAsync(d, s);
   return st;
+}
+
+dtfe_status_t dtfe_grid(dtfe_mesh_t h, int G, double box_len, const double center[3],
+                        unsigned ss, uint64_t seed, double* grid) {
+  return dtfe_grid_ex(h, G, box_len, center, ss, seed, DTFE_FP64, grid);
+}
+
+dtfe_status_t dtfe_grid_device(dtfe_mesh_t h, int G, double box_len, const double center[3],
+                               unsigned ss, uint64_t seed, int precision, double* d_grid,
+                               void* stream) {
+  SDTFE_TRY(check_grid(h, G, box_len, center, ss, precision));
+  if (!d_grid) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m.stream;
+  return launch_grid(m, G, box_len, center, ss, seed, precision, d_grid, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -510,7 +551,8 @@ void interpolate_to_3d_grid(double* particle_data, int n_particles, int* tetra_d
       DTFE_OK)
     return report("interpolate_to_3d_grid");
   const double c[3] = {center_x, center_y, center_z};
-  if (dtfe_grid(h, grid_dim, box_len, c, supersampling, call_seed(), grid) != DTFE_OK)
+  if (dtfe_grid_ex(h, grid_dim, box_len, c, supersampling, call_seed(),
+                   dtfe_get_default_precision(), grid) != DTFE_OK)
     report("interpolate_to_3d_grid");
   dtfe_mesh_destroy(h);
 }
@@ -526,7 +568,9 @@ void compute_3d_density(double* particle_data, int n_particles, int* tetra_data,
   if (s == DTFE_OK)
     for (int i = 0; i < n_particles; ++i) particle_data[4 * (size_t)i + 3] = dens[i];
   const double c[3] = {center_x, center_y, center_z};
-  if (s == DTFE_OK) s = dtfe_grid(h, grid_dim, box_len, c, supersampling, call_seed(), rho);
+  if (s == DTFE_OK)
+    s = dtfe_grid_ex(h, grid_dim, box_len, c, supersampling, call_seed(),
+                     dtfe_get_default_precision(), rho);
   if (s != DTFE_OK) report("compute_3d_density");
   dtfe_mesh_destroy(h);
 }
@@ -623,6 +667,13 @@ int* copy_fh_triangles(int* tetra_data, int n_tetra, double* particle_data, int 
 
 int* triangulate(double* particle_data, int n_particles, size_t* num_facets, const char* options) {
   if (num_facets) *num_facets = 0;
+  size_t cached_nt = 0;
+  if (particle_data && n_particles > 0) {
+    if (int* hit = tri_cache_lookup(particle_data, n_particles, options, &cached_nt)) {
+      if (num_facets) *num_facets = cached_nt;
+      return hit;
+    }
+  }
   if (!g_tri_fn) {
     set_error(DTFE_ERR_NO_TRIANGULATOR, "no Qhull backend registered (dtfe_set_triangulator)");
     fprintf(stderr, "TRIANGULATION ERROR: %s\n", dtfe_last_error());
@@ -641,6 +692,7 @@ int* triangulate(double* particle_data, int n_particles, size_t* num_facets, con
   if (tetra) dtfe_tetra_from_cells(particle_data, simp, nb, nt, tetra);
   free(simp);
   free(nb);
+  if (tetra) tri_cache_insert(particle_data, n_particles, options, tetra, nt);
   if (tetra && num_facets) *num_facets = nt;
   return tetra;
 }

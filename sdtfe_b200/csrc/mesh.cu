@@ -147,6 +147,19 @@ __global__ void k_gradients(const double4* __restrict__ pos, const int4* __restr
   grad[3 * (size_t)t + 2] = det3(xb, yb, rb, xc, yc, rc, xd, yd, rd) / den;
 }
 
+// Per-tet FP64 field of the mixed 3-D grid, the linear field of
+// src/triangulate.c:233-260 from vertex A expanded once per tet: the value at
+// (x, y, z) is k + gx x + gy y + gz z, k = rho_A - gx x_A - gy y_A - gz z_A.
+__global__ void k_field64(const double4* __restrict__ pos, const int4* __restrict__ rows,
+                          const double* __restrict__ grad, int nt, double4* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const int4 v = rows[2 * (size_t)t];
+  const double4 a = pos[v.x];
+  const double gx = grad[3 * (size_t)t], gy = grad[3 * (size_t)t + 1], gz = grad[3 * (size_t)t + 2];
+  out[t] = make_double4(a.w - gx * a.x - gy * a.y - gz * a.z, gx, gy, gz);
+}
+
 // Walk records for projection axis `axis`: positions and gradient permuted
 // cyclically, the neighbour links copied.  The FP64 record carries rho_A and
 // the gradient (the reference's field form); the FP32 record carries the four
@@ -557,6 +570,22 @@ dtfe_status_t mesh_gradients(Mesh* m) {
   return DTFE_OK;
 }
 
+dtfe_status_t mesh_field64(Mesh* m) {
+  if (m->fld64) return DTFE_OK;
+  if (!m->grad) return set_error(DTFE_ERR_INVALID, "mesh_field64 before mesh_gradients");
+  SDTFE_TRY(dmalloc_async(&m->fld64, m->nt, m));
+  if (m->nt) {
+    k_field64<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->grad, m->nt, m->fld64);
+    count_launch();
+  }
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    dfree_async(m->fld64, m->nt, m);
+    return set_error(DTFE_ERR_CUDA, "grid field: %s", cudaGetErrorString(e));
+  }
+  return DTFE_OK;
+}
+
 dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32) {
   if (axis < 0 || axis > 2) return set_error(DTFE_ERR_INVALID, "axis %d not in 0..2", axis);
   if (!m->grad) return set_error(DTFE_ERR_INVALID, "mesh_records before mesh_gradients");
@@ -729,6 +758,7 @@ void mesh_free(Mesh* m) {
     dfree_async(A.rec64, m->nt, m);
     dfree_async(A.rot32, 4 * (size_t)m->nt, m);
   }
+  dfree_async(m->fld64, m->nt, m);
   if (m->stream) cudaStreamSynchronize(m->stream);
   dfree(m->pos, m->n, m);
   dfree(m->rows, 2 * (size_t)m->nt, m);

@@ -69,6 +69,7 @@ struct Mesh {
   int4* rows = nullptr;     // 2 per tet: vertex ids, neighbour ids
   double* grad = nullptr;   // 3 per tet
   int* adj = nullptr;       // tets incident to each vertex
+  double4* fld64 = nullptr; // per-tet FP64 field (k, grad) of the mixed 3-D grid (on demand)
   AxisData ax[3];
   unsigned long long* stats = nullptr;  // kStatCount counters of the last map
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -77,12 +78,20 @@ struct Mesh {
   size_t bytes = 0;
 };
 
+// tricache.cc: triangulate()'s cache of results, keyed by the exact input.
+// lookup returns a malloc'd copy of the rows (nullptr: not cached).
+int* tri_cache_lookup(const double* xyz4, int n, const char* options, size_t* n_tetra);
+void tri_cache_insert(const double* xyz4, int n, const char* options, const int* tetra,
+                      size_t n_tetra);
+
 // mesh.cu
 dtfe_status_t mesh_upload(Mesh* m, const double* particle_data, int n, const int* tetra_data,
                           int nt, float p_mass, unsigned flags);
 dtfe_status_t mesh_density(Mesh* m);
 dtfe_status_t mesh_gradients(Mesh* m);
 dtfe_status_t mesh_records(Mesh* m, int axis, bool want64, bool want32);
+// the mixed 3-D grid's per-tet FP64 field (k_field64), built once on the mesh stream
+dtfe_status_t mesh_field64(Mesh* m);
 void mesh_drop_records(Mesh* m, int axis);
 // device bytes of one axis' walk records: held now, and still to build for a
 // map of the given precision
@@ -140,6 +149,8 @@ dtfe_status_t launch_trace32(Mesh& m, int axis, int n_rays, const double* d_x, c
 int num_map32_variants();
 void map32_variant_info(int i, int* block, int* minb, int* wide);
 dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
+                            uint64_t seed, int max_visits, double* d_grid, cudaStream_t s);
+dtfe_status_t launch_grid32(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
                             uint64_t seed, int max_visits, double* d_grid, cudaStream_t s);
 
 // Batched maps (walk.cu, walk32.cu): one persistent launch walks the tiles of

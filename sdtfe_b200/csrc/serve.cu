@@ -85,6 +85,7 @@ struct dtfe_server_s {
   dtfe_server_config_t cfg{};
   int device = 0;
   std::vector<dtfe_mesh_t> meshes;
+  bool auto_budget = false;  // device_budget follows the device's memory (config 0)
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request*> pending;
@@ -531,6 +532,23 @@ void free_server(Server* S) {
   delete S;
 }
 
+// The default budget: the device memory that is free now, less a reserve for
+// everything else on the device (other allocations, the CUDA context's
+// growth), plus what the server already accounts for (walk records of the
+// registered meshes, live maps), which is in use and so not in the free
+// figure.  Memory the record pool keeps for reuse counts as free: the
+// server's record builds draw on the same pool.
+dtfe_status_t set_auto_budget(Server* S) {
+  SDTFE_CUDA(cudaDeviceSynchronize());
+  mesh_trim_record_pool();
+  size_t fr = 0, total = 0;
+  SDTFE_CUDA(cudaMemGetInfo(&fr, &total));
+  const size_t reserve = std::max<size_t>(size_t(2) << 30, total / 20);
+  S->cfg.device_budget = (fr > reserve ? fr - reserve : 0) + S->in_use;
+  S->st.budget = S->cfg.device_budget;
+  return DTFE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -554,13 +572,8 @@ dtfe_status_t dtfe_server_create(const dtfe_server_config_t* cfg, dtfe_server_t*
   };
   cuda(cudaGetDevice(&S->device), "device");
   if (st == DTFE_OK && S->cfg.device_budget == 0) {
-    // memory the record pool keeps for reuse is free for this budget: the
-    // server's record builds draw on the same pool
-    cuda(cudaDeviceSynchronize(), "synchronise");
-    mesh_trim_record_pool();
-    size_t fr = 0, total = 0;
-    cuda(cudaMemGetInfo(&fr, &total), "memory info");
-    S->cfg.device_budget = fr / 4 * 3;
+    S->auto_budget = true;
+    st = set_auto_budget(S);
   }
   for (cudaStream_t* s : {&S->setup, &S->copy, &S->streams[0], &S->streams[1]})
     if (st == DTFE_OK) cuda(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "stream");
@@ -624,6 +637,7 @@ dtfe_status_t dtfe_server_add_mesh(dtfe_server_t S, dtfe_mesh_t mesh, int* mesh_
     r.last_use = ++S->use_clock;
     S->in_use += b;
   }
+  if (S->auto_budget) SDTFE_TRY(set_auto_budget(S));  // this mesh's records are in use, not free
   make_room(S, 0, {-1, -1});  // evict down to the budget (records of idle pairs only)
   note_use(S);
   *mesh_id = id;

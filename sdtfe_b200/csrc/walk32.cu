@@ -444,23 +444,82 @@ __device__ __forceinline__ T sel3(int k, T a, T b, T c) {
 
 struct FastStep {
   double z_out;    // exit crossing
-  double contrib;  // the chord's share of the integral
   float e_out;     // bound on the exit crossing's z error
   int next;        // record of the next tet; -1: the ray left the mesh here
+};
+
+// ---------------------------------------------------------------------------
+// What a walk does with each crossed tet.  An accumulator provides
+//   fast(...)        the fast step's chord, from the FP32 exit crossing and the
+//                    record's field; false declines the step (nothing committed)
+//   exact_exit(...)  whether the general step must recompute an FP32 exit
+//                    crossing exactly before its chord
+//   enter(z)         a ray's entry crossing was computed exactly
+//   general(...)     the general step's chord (FP64 field values)
+//   carry(leave)     the next tet is entered through this tet's leave face
+//                    (true) or, after a turn-around, its enter face (false)
+
+// Surface density (src/dtfe.c:356-369): the chord's value at its midpoint
+// times its length, when the midpoint lies strictly inside the slab.
+struct SurfaceAcc32 {
+  double sum = 0.0;
+
+  // The slab test compares the midpoint with a guard band (the crossings'
+  // error bounds); inside the band the step declines and the reference's FP64
+  // midpoint decides.  The chord value is the reference's own formula
+  // (src/dtfe.c:363-368) from the apex: the tet's linear field
+  // rho3 + grad . (p - v3) at the point p of the ray line at the chord's
+  // midpoint.  p lies on the line, so errors of the crossings only move chord
+  // ends, shared with the neighbours: they cancel to first order.
+  // fld = (rho3, grad_x, grad_y, grad_z); (x3, y3) = v3 - origin.  An exit
+  // through the hull (next == -1) is declined unless the error its FP32
+  // crossing can add to the chord is below 1e-7 of the ray's integral: such a
+  // crossing is not shared with a neighbouring chord, so its error does not
+  // cancel.
+  __device__ __forceinline__ bool fast(const MixConf& C, const RayState&, int, double z_in,
+                                       float e_in, double z_out, float e_out, int next,
+                                       const float4& f, float x3, float y3, float zw) {
+    const double d = z_out - z_in;
+    const double zm = z_in + 0.5 * d;
+    bool inside = true;
+    if (!(zm > C.zlo_in && zm < C.zhi_in)) {  // near a slab bound: this chord's own guard
+      const float g = 64.f * kEps * fabsf((float)zm) + e_in + e_out;
+      const float d0 = (float)(zm - C.z0d), d1 = (float)(zm - C.z1d);
+      if (!(fabsf(d0) > g && fabsf(d1) > g)) return false;  // the reference's midpoint decides
+      inside = d0 > 0.f && d1 < 0.f;
+    }
+    const float zr = (float)(zm - (double)zw);
+    const float g = __fmaf_rn(f.w, zr, __fmaf_rn(-f.z, y3, __fmaf_rn(-f.y, x3, f.x)));
+    const double contrib = inside ? (double)g * d : 0.0;
+    if (next == -1 && inside) {
+      // the exit crossing's z error times the field is not cancelled: at most
+      // about 1.7e-7 of the ray's integral (5/3 e_out)
+      if (!(fabsf(g) * e_out <= 1e-7f * (float)fabs(sum + contrib))) return false;
+    }
+    sum += contrib;
+    return true;
+  }
+  __device__ __forceinline__ bool exact_exit(double, float) const { return false; }
+  __device__ __forceinline__ void enter(double) {}
+  __device__ __forceinline__ void carry(bool) {}
+  __device__ __forceinline__ void general(const TetRot32* __restrict__ R, const MixConf& C,
+                                          const RayState& r, int t, int enter, int leave,
+                                          double z_in, double z_out, float hz, float e_inout,
+                                          int* fallbacks) {
+    sum += chord32(R, C, r, t, enter, leave, z_in, z_out, hz, e_inout, fallbacks);
+  }
 };
 
 // One walk step on the record of (tet, entry face), for a ray whose entry
 // crossing (z_in, f_in) was carried over from the previous tet.  Succeeds
 // when the FP32 products decide all six reference signs, the reference's rule
-// enters through the known face and the chord midpoint is clear of the slab
-// bounds; otherwise nothing is committed and the general step takes the tet.
-// The step also declines an ill-conditioned exit crossing, and an exit
-// through the hull (o->next = -1 on success) unless the error its FP32
-// crossing can add to the chord is below 1e-7 of the ray's integral (sum):
-// such a crossing is not shared with a neighbouring chord, so its error does
-// not cancel.  The general step computes those crossings exactly.
+// enters through the known face and the accumulator takes the chord
+// (SurfaceAcc32: the midpoint is clear of the slab bounds); otherwise nothing
+// is committed and the general step takes the tet.  The step also declines an
+// ill-conditioned exit crossing; the general step computes it exactly.
+template <class Acc>
 __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, int ri,
-                                          double z_in, float e_in, double sum, FastStep* o) {
+                                          double z_in, float e_in, Acc& acc, FastStep* o) {
   const TetRot32* p = C.rot + ri;
   const float4 a = __ldg(&p->xy01), b = __ldg(&p->xy23), z = __ldg(&p->z), f = __ldg(&p->fld);
   const int4 nb = __ldg(&p->nb);
@@ -510,35 +569,13 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
   // the rounding of the offset (the double sum with the apex z is exact).
   // The weights' error enters the offset's numerator and its denominator, so
   // the crossing is within 5/3 e_out (and the rounding) of the exact one; the
-  // slab test below compares the midpoint, whose error is at most half of
+  // slab test compares the midpoint, whose error is at most half of
   // e_in + e_out times 5/3, with the whole of e_in + e_out.
   const float e_out = (cond + 8.f * kEps) * fmaxf(fabsf(hi), fabsf(hj));
   const double z_out = (double)z.w + (double)dzr;
-  const double d = z_out - z_in;
-  const double zm = z_in + 0.5 * d;
-  bool inside = true;
-  if (!(zm > C.zlo_in && zm < C.zhi_in)) {  // near a slab bound: this chord's own guard
-    const float g = 64.f * kEps * fabsf((float)zm) + e_in + e_out;
-    const float d0 = (float)(zm - C.z0d), d1 = (float)(zm - C.z1d);
-    if (!(fabsf(d0) > g && fabsf(d1) > g)) return false;  // the reference's midpoint decides
-    inside = d0 > 0.f && d1 < 0.f;
-  }
-  // the reference's chord value (src/dtfe.c:363-368) from the apex: the
-  // tet's linear field rho3 + grad . (p - v3) at the point p of the ray line
-  // at the chord's midpoint.  p lies on the line, so errors of the crossings
-  // only move chord ends, shared with the neighbours: they cancel to first
-  // order.  fld = (rho3, grad_x, grad_y, grad_z); (x3, y3) = v3 - origin.
-  const float zr = (float)(zm - (double)z.w);
-  const float g = __fmaf_rn(f.w, zr, __fmaf_rn(-f.z, y3, __fmaf_rn(-f.y, x3, f.x)));
-  const double contrib = inside ? (double)g * d : 0.0;
-  if (next == -1 && inside) {
-    // the exit crossing's z error times the field is not cancelled: at most
-    // about 1.7e-7 of the ray's integral (5/3 e_out)
-    if (!(fabsf(g) * e_out <= 1e-7f * (float)fabs(sum + contrib))) return false;
-  }
+  if (!acc.fast(C, r, ri >> 2, z_in, e_in, z_out, e_out, next, f, x3, y3, z.w)) return false;
   o->z_out = z_out;
   o->e_out = e_out;
-  o->contrib = contrib;
   o->next = next;
   return true;
 }
@@ -552,10 +589,100 @@ __device__ __forceinline__ int rot_next(const MixConf& C, int t, int m) {
   return v >= 0 ? v : -1;
 }
 
+// 3-D grid column (src/dtfe.c:465-513): the tet's linear field is sampled at
+// the fine z nodes inside each chord and added, with weight 1/ss^3, to the
+// node's cell of the column.  Node k sits at z0 + dzs k + dzs/2; a chord
+// [z_in, z_out] holds the nodes from the reference's index of z_in up to,
+// not including, that of z_out (clamped to [0, nzs)).  Which chord a node
+// belongs to must be the FP64 path's: the entry crossing is shared with the
+// previous chord, so the index carried from there is used, and an FP32 exit
+// crossing whose error band holds a node is recomputed exactly (the fast
+// step declines; the general step asks for the exact crossing).  Nodes of
+// the hull exit always use the exact crossing.  Node values are FP64: a
+// point value has no neighbouring chord to cancel its error against, and the
+// FP32 linear field loses up to the tet's density contrast in relative
+// precision, so the fast step evaluates the per-tet FP64 field k_field64
+// built (k + gx x + gy y + gz z) and the general step the reference's own
+// expression from vertex A.
+struct ColumnAcc32 {
+  double* col;          // the column's cells (z fastest)
+  const double4* __restrict__ fld;  // per-tet FP64 field (mesh_field64)
+  double z0, dzs, inv_dzs, w;
+  int nzs, ss;
+  int i_in;             // index of the first node of the next chord (clamped to [-1, nzs + 1])
+  int i_out;            // the general step's exit index
+
+  // the reference's index expression (src/dtfe.c:493-496), kept in int range
+  __device__ __forceinline__ int node_index(double z) const {
+    const double t = ceil((z - z0 - dzs / 2.) / dzs);
+    return (int)fmin(fmax(t, -1.0), (double)nzs + 1.0);
+  }
+  // True when a node with an index in [0, nzs) may lie on the other side of
+  // an FP32 crossing z (error bound e, 5/3 e and the FP64 rounding covered
+  // by 2e plus 64 ulps).  *t receives the node coordinate of z.
+  __device__ __forceinline__ bool near_node(double z, float e, double* t) const {
+    *t = (z - z0 - dzs / 2.) * inv_dzs;
+    const double fl = floor(*t);
+    const double band = (2.0 * (double)e + 64.0 * DBL_EPSILON * (fabs(z) + fabs(z0) + dzs)) * inv_dzs;
+    return fl >= -1.0 && fl < (double)nzs && (*t - fl <= band || fl + 1.0 - *t <= band);
+  }
+  __device__ __forceinline__ bool fast(const MixConf&, const RayState& r, int t, double,
+                                       float, double z_out, float e_out, int next, const float4&,
+                                       float, float, float) {
+    if (next < 0) return false;  // the hull exit: its crossing is computed exactly
+    double tz;
+    if (near_node(z_out, e_out, &tz)) return false;
+    // away from the band tz's ceiling is the reference's index of z_out
+    const int i1u = (int)fmin(fmax(ceil(tz), -1.0), (double)nzs + 1.0);
+    const int i0 = i_in < 0 ? 0 : i_in, i1 = i1u > nzs ? nzs : i1u;
+    if (i1 > i0) {
+      const double2 kx = __ldg(reinterpret_cast<const double2*>(fld + t));
+      const double2 yz = __ldg(reinterpret_cast<const double2*>(fld + t) + 1);
+      const double base = kx.x + kx.y * r.ox + yz.x * r.oy;
+      for (int is = i0; is < i1; ++is) {
+        const int iz = (int)((unsigned)is / (unsigned)ss);
+        const double zi = z0 + dzs * is + dzs / 2.;
+        col[iz] += (base + yz.y * zi) * w;
+      }
+    }
+    i_in = i1u;
+    return true;
+  }
+  __device__ __forceinline__ bool exact_exit(double z_out, float e_out) const {
+    double t;
+    return near_node(z_out, e_out, &t);
+  }
+  __device__ __forceinline__ void enter(double z_in) { i_in = node_index(z_in); }
+  __device__ __forceinline__ void carry(bool through_leave) {
+    if (through_leave) i_in = i_out;  // else the enter face's index, already in i_in
+  }
+  __device__ __forceinline__ void general(const TetRot32* __restrict__, const MixConf& C,
+                                          const RayState& r, int t, int, int, double, double z_out,
+                                          float, float, int* fallbacks) {
+    i_out = node_index(z_out);
+    const int i0 = i_in < 0 ? 0 : i_in, i1 = i_out > nzs ? nzs : i_out;
+    if (i1 <= i0) return;
+    // the reference's FP64 value (src/dtfe.c:498-512), grid along z (no permutation)
+    const int4 v = __ldg(&C.rows[2 * (size_t)t]);
+    const double4 A = C.pos[v.x];
+    const double gx = C.grad[3 * (size_t)t], gy = C.grad[3 * (size_t)t + 1],
+                 gz = C.grad[3 * (size_t)t + 2];
+    const double fixed = A.w + gx * (r.ox - A.x) + gy * (r.oy - A.y) - gz * A.z;
+    for (int is = i0; is < i1; ++is) {
+      const int iz = (int)((unsigned)is / (unsigned)ss);
+      const double zi = z0 + dzs * is + dzs / 2.;
+      col[iz] += (fixed + gz * zi) * w;
+    }
+    ++*fallbacks;
+  }
+};
+
 // State of one ray between steps.
+template <class Acc>
 struct WalkState {
   RayState r;
-  double sum, z_in;
+  Acc acc;
+  double z_in;
   float e_in;        // bound on z_in's error
   uint64_t ctr;      // perturbation draws so far
   int crossed, fallbacks, cur, prev, ri;
@@ -572,9 +699,10 @@ constexpr int kWalkOn = -1;  // general_step: the walk continues
 // Returns kWalkOn, or the ray's final status.  Kept out of line: it runs on
 // about one step in a hundred and would otherwise crowd the fast loop's
 // registers.
+template <class Acc>
 __device__ __noinline__ int general_step(const TetRot32* __restrict__ R, const MixConf& C,
                                          uint64_t ray, const unsigned char* __restrict__ lut,
-                                         WalkState& w, int* visits, int max_record) {
+                                         WalkState<Acc>& w, int* visits, int max_record) {
   RayState& r = w.r;
   const int cur = w.cur;
   int4 nb;
@@ -614,23 +742,28 @@ __device__ __noinline__ int general_step(const TetRot32* __restrict__ R, const M
   if (!w.carried || nb_at(nb, enter) != w.prev) {
     w.z_in = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, enter, r.ox, r.oy);
     w.e_in = 0.f;
+    w.acc.enter(w.z_in);
     ++w.fallbacks;
   }
   // exit crossing: FP32 unless it leaves the mesh (not shared with a
-  // neighbouring chord) or is ill-conditioned
+  // neighbouring chord), is ill-conditioned, or the accumulator needs it exact
   float dzo, e_out = 0.f;
   double z_out;
   const float cond = crossing(leave, u, bmax, v, &dzo);
   const float hz = fmaxf(fmaxf(fabsf(v.z[1] - v.z[0]), fabsf(v.z[2] - v.z[0])),
                          fabsf(v.z[3] - v.z[0]));
-  if (nb_at(nb, leave) == -1 || !(cond <= kCrossingTol)) {
-    z_out = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
-    ++w.fallbacks;
-  } else {
+  bool exact_out = nb_at(nb, leave) == -1 || !(cond <= kCrossingTol);
+  if (!exact_out) {
     z_out = (double)v.z[0] + (double)dzo;
     e_out = (cond + 8.f * kEps) * hz;
+    exact_out = w.acc.exact_exit(z_out, e_out);
   }
-  w.sum += chord32(R, C, r, cur, enter, leave, w.z_in, z_out, hz, w.e_in + e_out, &w.fallbacks);
+  if (exact_out) {
+    z_out = exact_crossing(R, C.rec64, C.exact32, C.lz, cur, leave, r.ox, r.oy);
+    e_out = 0.f;
+    ++w.fallbacks;
+  }
+  w.acc.general(R, C, r, cur, enter, leave, w.z_in, z_out, hz, w.e_in + e_out, &w.fallbacks);
 
   // move on (src/dtfe.c:300-309)
   int m = leave;
@@ -644,6 +777,7 @@ __device__ __noinline__ int general_step(const TetRot32* __restrict__ R, const M
     w.z_in = z_out;
     w.e_in = e_out;
   }  // else the enter face's crossing, already in z_in
+  w.acc.carry(m == leave);
   w.carried = true;
   w.ri = rot_next(C, cur, m);
   w.prev = cur;
@@ -652,19 +786,19 @@ __device__ __noinline__ int general_step(const TetRot32* __restrict__ R, const M
 }
 
 // The mixed walk.  Same control flow as walk64 (src/dtfe.c:247-374); returns
-// the status, the integral in *rho and the crossing count.  A tet entered
-// through a known face, with the crossing there in hand, takes the fast step
-// on its record for that entry face; any tet the fast step declines takes the
-// general step.  The first tet is entered through the hull triangle the
-// sample was located in (ft_tri; its face is known from the hull build), at
-// the exact crossing.
-__device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixConf& C, int ft,
-                                      int ft_tri, double x, double y, uint64_t ray,
-                                      const unsigned char* __restrict__ lut, double* rho_out,
-                                      int* crossed_out, int* fallbacks_out, int* visits,
-                                      int max_record) {
+// the status and the crossing count, and hands each crossed tet's chord to
+// the accumulator.  A tet entered through a known face, with the crossing
+// there in hand, takes the fast step on its record for that entry face; any
+// tet the fast step declines takes the general step.  The first tet is
+// entered through the hull triangle the sample was located in (ft_tri; its
+// face is known from the hull build), at the exact crossing.
+template <class Acc>
+__device__ __forceinline__ int walk_mixed(const TetRot32* __restrict__ R, const MixConf& C, int ft,
+                                          int ft_tri, double x, double y, uint64_t ray,
+                                          const unsigned char* __restrict__ lut, Acc& acc,
+                                          int* crossed_out, int* fallbacks_out, int* visits,
+                                          int max_record) {
   *crossed_out = 0;
-  *rho_out = 0.0;
   *fallbacks_out = 0;
   if (ft < 0) return kRayMiss;
   RayState r;
@@ -672,7 +806,7 @@ __device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixC
   r.oy = y;
   ray_setup(r, C);
   uint64_t ctr = 0;
-  double sum = 0.0, z_in = 0.0;
+  double z_in = 0.0;
   float e_in = 0.f;
   bool carried = false;
   int crossed = 0, fallbacks = 0;
@@ -682,6 +816,7 @@ __device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixC
   if (C.rot && ft_tri >= 0) {  // enter through the located hull face, exactly
     const int F = C.tri_face[ft_tri];
     z_in = exact_crossing(R, C.rec64, C.exact32, C.lz, ft, F, r.ox, r.oy);
+    acc.enter(z_in);
     ++fallbacks;
     carried = true;
     ri = 4 * ft + F;
@@ -693,10 +828,9 @@ __device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixC
     }
     if (ri >= 0) {
       FastStep o;
-      if (fast_step(C, r, ri, z_in, e_in, sum, &o)) {
+      if (fast_step(C, r, ri, z_in, e_in, acc, &o)) {
         if (visits != nullptr && crossed < max_record) visits[crossed] = cur;
         ++crossed;
-        sum += o.contrib;
         if (o.next < 0) {  // left the mesh
           status = kRayOk;
           break;
@@ -709,9 +843,9 @@ __device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixC
         continue;
       }
     }
-    WalkState w;
+    WalkState<Acc> w;
     w.r = r;
-    w.sum = sum;
+    w.acc = acc;
     w.z_in = z_in;
     w.e_in = e_in;
     w.ctr = ctr;
@@ -724,7 +858,7 @@ __device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixC
     w.carried = carried && crossed > 0;
     status = general_step(R, C, ray, lut, w, visits, max_record);
     r = w.r;
-    sum = w.sum;
+    acc = w.acc;
     z_in = w.z_in;
     e_in = w.e_in;
     ctr = w.ctr;
@@ -739,8 +873,21 @@ __device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixC
   // as the reference (and walk64): a ray that fails reports no crossings, so
   // that the pixel mean leaves it out
   *crossed_out = status == kRayOk ? crossed : 0;
-  *rho_out = status == kRayOk ? sum : 0.0;
   *fallbacks_out = fallbacks;
+  return status;
+}
+
+// The surface-density walk: the ray's integral in *rho_out (0 unless the
+// ray's status is kRayOk).
+__device__ __forceinline__ int walk32(const TetRot32* __restrict__ R, const MixConf& C, int ft,
+                                      int ft_tri, double x, double y, uint64_t ray,
+                                      const unsigned char* __restrict__ lut, double* rho_out,
+                                      int* crossed_out, int* fallbacks_out, int* visits,
+                                      int max_record) {
+  SurfaceAcc32 acc;
+  const int status = walk_mixed(R, C, ft, ft_tri, x, y, ray, lut, acc, crossed_out, fallbacks_out,
+                                visits, max_record);
+  *rho_out = status == kRayOk ? acc.sum : 0.0;
   return status;
 }
 
@@ -1006,6 +1153,61 @@ __global__ void __launch_bounds__(128) k_trace32(const TetRot32* __restrict__ re
   status[i] = st;
 }
 
+// 3-D grid (src/dtfe.c:658-735) on the mixed walk: one thread per column
+// (i along x, j along y), its ss^2 sub-rays in (is, js) order at the
+// reference's positions, each located on the projected hull from triangle 0
+// and walked with ColumnAcc32.  No two threads touch the same column.
+struct GridArgs32 {
+  const TetRot32* __restrict__ rec;
+  const TriRec64* __restrict__ tri;
+  int n_tri, G, ss, loc_budget;
+  double dxy, offx, offy;
+  double z0, dzs, inv_dzs, w;
+  MixConf C;
+  const double4* __restrict__ fld;
+  double* __restrict__ grid;
+  unsigned long long* __restrict__ stats;
+};
+
+__global__ void __launch_bounds__(128) k_grid32(const __grid_constant__ GridArgs32 a) {
+  __shared__ unsigned char s_lut[kLutBytes];
+  fill_lut(s_lut);
+  __syncthreads();
+  const long long cidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = cidx < (long long)a.G * a.G;
+  int worst = kRayOk, visits = 0, fallbacks = 0;
+  if (active) {
+    const int i = (int)(cidx / a.G), j = (int)(cidx % a.G);
+    const double ds = a.dxy / a.ss;
+    ColumnAcc32 acc;
+    acc.col = a.grid + (size_t)cidx * a.G;
+    acc.fld = a.fld;
+    acc.z0 = a.z0;
+    acc.dzs = a.dzs;
+    acc.inv_dzs = a.inv_dzs;
+    acc.w = a.w;
+    acc.nzs = a.G * a.ss;
+    acc.ss = a.ss;
+    acc.i_in = 0;
+    acc.i_out = 0;
+    for (int is = 0; is < a.ss; ++is)
+      for (int js = 0; js < a.ss; ++js) {
+        const double x = i * a.dxy + a.offx + is * ds + ds / 2.;
+        const double y = j * a.dxy + a.offy + js * ds + ds / 2.;
+        int st = kRayMiss, c = 0, fb = 0, ft_tri = -1;
+        const int ft = a.n_tri > 0 ? locate64(a.tri, 0, x, y, a.loc_budget, &st, &ft_tri) : -1;
+        if (ft >= 0) {
+          const uint64_t rid = ((uint64_t)cidx * a.ss + (uint64_t)is) * a.ss + (uint64_t)js;
+          st = walk_mixed(a.rec, a.C, ft, ft_tri, x, y, rid, s_lut, acc, &c, &fb, nullptr, 0);
+        }
+        visits += c;
+        fallbacks += fb;
+        if (st > worst) worst = st;
+      }
+  }
+  add_stats32(a.stats, active, visits, worst, fallbacks);
+}
+
 MixConf mix_conf(const Mesh& m, int axis, double z0, double lz, double dist, uint64_t seed,
                  int max_visits) {
   MixConf C;
@@ -1152,6 +1354,46 @@ dtfe_status_t launch_map32(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   const cudaError_t e = cudaGetLastError();
   scratch_free_async(loc, s);
   SDTFE_CUDA(e);
+  SDTFE_CUDA(cudaEventRecord(m.ev1, s));
+  m.timed = true;
+  return DTFE_OK;
+}
+
+dtfe_status_t launch_grid32(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
+                            uint64_t seed, int max_visits, double* d_grid, cudaStream_t s) {
+  SDTFE_TRY(check_mixed(m, DTFE_AXIS_Z));
+  const AxisData& A = m.ax[DTFE_AXIS_Z];
+  if (A.n_tri >= (1 << 27))
+    return set_error(DTFE_ERR_UNSUPPORTED, "grids over %d hull triangles (at most 2^27 - 1)", A.n_tri);
+  if ((long long)G * ss > (1LL << 30))
+    return set_error(DTFE_ERR_UNSUPPORTED, "grid_dim %d x supersampling %u: too many nodes", G, ss);
+  GridArgs32 a;
+  a.rec = A.rot32;
+  a.tri = A.tri;
+  a.n_tri = A.n_tri;
+  a.G = G;
+  a.ss = (int)ss;
+  a.loc_budget = 4 * A.n_tri + 64;
+  // src/dtfe.c:668-735 and :398-404: cell and node spacing, weight 1/ss^3
+  a.dxy = box_len / G;
+  a.offx = -(box_len / 2.0) + center[0];
+  a.offy = -(box_len / 2.0) + center[1];
+  a.z0 = -(box_len / 2.0) + center[2];
+  const double dz = box_len / G;
+  a.dzs = dz / ss;
+  a.inv_dzs = 1.0 / a.dzs;
+  a.w = 1. / ((unsigned)ss * (unsigned)ss * (unsigned)ss);
+  a.C = mix_conf(m, DTFE_AXIS_Z, a.z0, box_len, (a.dxy / 2.0) / kPerturbMax, seed, max_visits);
+  if (!m.fld64) return set_error(DTFE_ERR_INVALID, "mixed grid before its FP64 field");
+  a.fld = m.fld64;
+  a.grid = d_grid;
+  a.stats = m.stats;
+  const long long ncol = (long long)G * G;
+  SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
+  SDTFE_CUDA(cudaEventRecord(m.ev0, s));
+  k_grid32<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(a);
+  count_launch();
+  SDTFE_CUDA(cudaGetLastError());
   SDTFE_CUDA(cudaEventRecord(m.ev1, s));
   m.timed = true;
   return DTFE_OK;

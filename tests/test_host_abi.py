@@ -191,3 +191,87 @@ def test_mesh_create_reports_cuda_failure_without_gpu():
     pos4 = to_pos4(np.random.default_rng(0).random((10, 3)))
     with pytest.raises(DTFEError):
         Mesh(pos4, np.zeros((1, 8), np.int32))
+
+
+def test_triangulate_cache_answers_repeated_inputs_without_the_backend():
+    """triangulate() keeps its results keyed by the exact input: a repeated
+    input gets the same rows without a backend call; one changed coordinate
+    or other options run the backend again; column 3 plays no part; a zero
+    limit disables the cache."""
+    from scipy.spatial import Delaunay
+
+    from oracle.oracle import to_pos4
+    from sdtfe_b200 import lib
+
+    L = lib()
+    libc = ctypes.CDLL(None)
+    libc.malloc.restype = ctypes.c_void_p
+    libc.malloc.argtypes = [ctypes.c_size_t]
+    libc.free.argtypes = [ctypes.c_void_p]
+    L.triangulate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t),
+                              ctypes.c_char_p]
+    L.triangulate.restype = ctypes.c_void_p
+    FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p,
+                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p),
+                          ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p)
+    calls = [0]
+
+    def backend(xyz4, n, options, simp, nbr, nt, user):
+        calls[0] += 1
+        pts = np.ctypeslib.as_array(ctypes.cast(xyz4, ctypes.POINTER(ctypes.c_double)),
+                                    shape=(n, 4))[:, :3].copy()
+        d = Delaunay(pts, qhull_options="Qt Qbb Qz")
+        for arr, out in ((d.simplices, simp), (d.neighbors, nbr)):
+            a = np.ascontiguousarray(arr, np.int32)
+            p = libc.malloc(a.nbytes)
+            ctypes.memmove(p, a.ctypes.data, a.nbytes)
+            out[0] = p
+        nt[0] = len(d.simplices)
+        return 0
+
+    def tri(pos4, options=b"qhull d Qz Qt Qbb"):
+        nf = ctypes.c_size_t(0)
+        ptr = L.triangulate(pos4.ctypes.data, len(pos4), ctypes.byref(nf), options)
+        assert ptr and nf.value > 0
+        rows = np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_int)),
+                                     shape=(nf.value, 8)).copy()
+        libc.free(ptr)
+        return rows
+
+    def stats():
+        h, m = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        e, b = ctypes.c_size_t(), ctypes.c_size_t()
+        L.dtfe_triangulation_cache_stats(ctypes.byref(h), ctypes.byref(m), ctypes.byref(e),
+                                         ctypes.byref(b))
+        return h.value, m.value, e.value, b.value
+
+    cb = FN(backend)
+    L.dtfe_set_triangulator.argtypes = [FN, ctypes.c_void_p]
+    L.dtfe_set_triangulator(cb, None)
+    try:
+        L.dtfe_set_triangulation_cache(0)  # start empty
+        L.dtfe_set_triangulation_cache(64 << 20)
+        h0, m0, _, _ = stats()
+        pos4 = to_pos4(np.random.default_rng(9).random((400, 3)))
+        first = tri(pos4)
+        assert calls[0] == 1
+        again = pos4.copy()
+        again[:, 3] = 7.5  # column 3 is not part of the key
+        assert np.array_equal(tri(again), first) and calls[0] == 1
+        h, m, entries, nbytes = stats()
+        assert (h - h0, m - m0, entries) == (1, 1, 1)
+        assert nbytes == 400 * 3 * 8 + first.size * 4
+        moved = pos4.copy()
+        moved[17, 1] = np.nextafter(moved[17, 1], 2.0)
+        tri(moved)
+        assert calls[0] == 2
+        tri(pos4, b"qhull d Qz Qt Qbb Pp")
+        assert calls[0] == 3
+        assert np.array_equal(tri(pos4), first) and calls[0] == 3
+        L.dtfe_set_triangulation_cache(0)
+        assert stats()[2] == 0
+        assert np.array_equal(tri(pos4), first) and calls[0] == 4
+    finally:
+        L.dtfe_set_triangulation_cache(1024 << 20)
+        L.dtfe_set_triangulator.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.dtfe_set_triangulator(None, None)
