@@ -45,6 +45,7 @@
 // Compiled with -fmad=false like walk.cu: the sample positions and the point
 // location it shares with the FP64 walk must round as the reference does;
 // the FP32 arithmetic asks for fused multiply-adds explicitly.
+#include <algorithm>
 #include <cfloat>
 #include <cstring>
 
@@ -1060,24 +1061,33 @@ __global__ void __launch_bounds__(128) k_locate_map32(const __grid_constant__ Ma
 // across every job of the batch (maps of different meshes, sides and sample
 // counts), so uneven maps share the GPU without a tail per map.  Job j owns
 // global tiles [first[j], first[j+1]) and maps them to its own tiles
-// [tile0, tile0 + count).  The job's arguments are staged in shared memory.
-// Thread 0 claims the next tile (and finds its job) while the block walks the
-// current one, so the claim's latency is hidden.
-__device__ __forceinline__ void claim_tile(const BatchJob32* __restrict__ jobs, int n_jobs,
-                                           unsigned long long* __restrict__ queue,
-                                           long long* tile, int* job) {
-  const long long t = (long long)atomicAdd(queue, 1ull);
-  int lo = 0, hi = n_jobs - 1;  // last job whose first tile <= t
+// [tile0, tile0 + count).  The job table travels as the kernel's own
+// parameter (up to kMaxJobsPerLaunch32 jobs; larger batches are launched in
+// chunks): a tile's job is found by a binary search over the table with a
+// block-uniform index, and the walk reads its job's fields from the constant
+// bank as k_map32 reads its single map's, instead of holding them in
+// registers.  Thread 0 claims the next tile while the block walks the current
+// one, so the claim's latency is hidden.
+constexpr int kMaxJobsPerLaunch32 = 96;
+struct BatchTable32 {
+  int n_jobs;
+  long long total_tiles;
+  BatchJob32 jobs[kMaxJobsPerLaunch32];
+};
+static_assert(sizeof(BatchTable32) <= 32764, "the job table must fit the kernel parameter space");
+
+__device__ __forceinline__ int job_of(const BatchTable32& P, long long t) {
+  int lo = 0, hi = P.n_jobs - 1;  // last job whose first tile <= t
   while (lo < hi) {
     const int mid = (lo + hi + 1) / 2;
-    if (__ldg(&jobs[mid].first) <= t) lo = mid;
+    if (P.jobs[mid].first <= t) lo = mid;
     else hi = mid - 1;
   }
-  *tile = t;
-  *job = lo;
+  return lo;
 }
 
-// The same for the global tiles of a batch (loc indexed by global tile).
+// Every tile's shared point location, one thread per tile, before the batch
+// kernel (loc indexed by global tile; jobs in device memory).
 __global__ void __launch_bounds__(128) k_locate_batch32(const BatchJob32* __restrict__ jobs,
                                                         int n_jobs, long long total_tiles,
                                                         int2* __restrict__ loc) {
@@ -1094,36 +1104,26 @@ __global__ void __launch_bounds__(128) k_locate_batch32(const BatchJob32* __rest
 
 template <int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB)
-    k_batch32(const BatchJob32* __restrict__ jobs, int n_jobs, long long total_tiles,
-              unsigned long long* __restrict__ queue, const int2* __restrict__ loc) {
+    k_batch32(const __grid_constant__ BatchTable32 P, unsigned long long* __restrict__ queue,
+              const int2* __restrict__ loc) {
   extern __shared__ double s_val32[];
   __shared__ unsigned char s_lut[kLutBytes];
-  __shared__ MapArgs32 s_args;
   __shared__ long long s_tile[2];
-  __shared__ int s_job[2];
   fill_lut(s_lut);
-  if (threadIdx.x == 0) claim_tile(jobs, n_jobs, queue, &s_tile[0], &s_job[0]);
+  if (threadIdx.x == 0) s_tile[0] = (long long)atomicAdd(queue, 1ull);
   __syncthreads();
-  int cur_job = -1;
   for (int it = 0;; ++it) {
     const int slot = it & 1;
     const long long tile = s_tile[slot];
-    const int j = s_job[slot];
-    if (tile >= total_tiles) break;
+    if (tile >= P.total_tiles) break;
     // the next claim goes to the other slot, read only after the end-of-tile barrier
-    if (threadIdx.x == 0) claim_tile(jobs, n_jobs, queue, &s_tile[slot ^ 1], &s_job[slot ^ 1]);
-    if (j != cur_job) {  // stage the job's arguments (j is the same for the whole block)
-      const int* src = reinterpret_cast<const int*>(&jobs[j].args);
-      int* dst = reinterpret_cast<int*>(&s_args);
-      for (int k = threadIdx.x; k < (int)(sizeof(MapArgs32) / sizeof(int)); k += BLOCK)
-        dst[k] = src[k];
-      cur_job = j;
-      __syncthreads();
-    }
-    unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + s_args.TW * s_args.TH * s_args.S);
-    map_tile32<BLOCK>(s_args, jobs[j].tile0 + (int)(tile - jobs[j].first), loc + tile, s_lut,
+    if (threadIdx.x == 0) s_tile[slot ^ 1] = (long long)atomicAdd(queue, 1ull);
+    const int j = job_of(P, tile);
+    const MapArgs32& a = P.jobs[j].args;
+    unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val32 + a.TW * a.TH * a.S);
+    map_tile32<BLOCK>(a, P.jobs[j].tile0 + (int)(tile - P.jobs[j].first), loc + tile, s_lut,
                       s_val32, s_ok);
-    __syncthreads();  // s_val, s_args and the claimed slot are reused next
+    __syncthreads();  // s_val and the claimed slot are reused next
   }
 }
 
@@ -1276,7 +1276,7 @@ const Variant32 kVariants32[] = {
 constexpr int kNumVariants32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
 constexpr int kDefaultVariant32 = 7;  // (128, 8): the usual winner on B200
 
-typedef void (*BatchKernel32)(const BatchJob32*, int, long long, unsigned long long*, const int2*);
+typedef void (*BatchKernel32)(const BatchTable32, unsigned long long*, const int2*);
 const BatchKernel32 kBatch32[] = {k_batch32<256, 2>, k_batch32<256, 3>, k_batch32<256, 4>,
                                   k_batch32<128, 4>, k_batch32<128, 6>, k_batch32<256, 2>,
                                   k_batch32<256, 3>, k_batch32<128, 8>, k_batch32<64, 16>,
@@ -1488,9 +1488,26 @@ dtfe_status_t launch_batch32(const BatchPlan& plan, const void* d_jobs, unsigned
   k_locate_batch32<<<(unsigned)((plan.total_tiles + 127) / 128), 128, 0, s>>>(
       jobs, plan.n_jobs, plan.total_tiles, static_cast<int2*>(d_loc));
   count_launch();
-  kBatch32[vi]<<<grid, kVariants32[vi].block, plan.smem, s>>>(
-      jobs, plan.n_jobs, plan.total_tiles, d_queue, static_cast<const int2*>(d_loc));
-  count_launch();
+  // the job table as the kernel's parameter, kMaxJobsPerLaunch32 jobs per
+  // launch; each chunk's tiles are renumbered from 0 and pull from the queue
+  // counter, cleared before each chunk (the caller clears it for the first)
+  const BatchJob32* host = reinterpret_cast<const BatchJob32*>(plan.jobs.data());
+  static thread_local BatchTable32 P;  // about 30 KB: not on the stack
+  for (int j0 = 0; j0 < plan.n_jobs; j0 += kMaxJobsPerLaunch32) {
+    const int n = std::min(kMaxJobsPerLaunch32, plan.n_jobs - j0);
+    const long long base = host[j0].first;
+    const long long end = j0 + n < plan.n_jobs ? host[j0 + n].first : plan.total_tiles;
+    P.n_jobs = n;
+    P.total_tiles = end - base;
+    for (int k = 0; k < n; ++k) {
+      P.jobs[k] = host[j0 + k];
+      P.jobs[k].first -= base;
+    }
+    if (j0 > 0) SDTFE_CUDA(cudaMemsetAsync(d_queue, 0, sizeof(unsigned long long), s));
+    kBatch32[vi]<<<grid, kVariants32[vi].block, plan.smem, s>>>(
+        P, d_queue, static_cast<const int2*>(d_loc) + base);
+    count_launch();
+  }
   SDTFE_CUDA(cudaGetLastError());
   return DTFE_OK;
 }

@@ -84,6 +84,29 @@ def test_batch_matches_single_maps(sd, torch_cuda, cutouts, precision, flags):
     b.close()
 
 
+def test_batch_larger_than_one_job_table(sd, torch_cuda, cutouts):
+    """A mixed batch of 150 small maps: more jobs than one launch's parameter
+    table holds (96), so it runs in chunks, each with its own tile numbering
+    and queue; every map equal to dtfe_map, captured in a graph and not."""
+    torch = torch_cuda
+    rng = np.random.default_rng(31)
+    jobs = [(int(rng.integers(len(cutouts))), int(rng.choice([16, 24, 40])),
+             int(rng.integers(1, 9)), int(rng.integers(3))) for _ in range(150)]
+    params = [_params(sd, G, S, ax, 1, 5000 + k) for k, (_, G, S, ax) in enumerate(jobs)]
+    want = [cutouts[mi].map(p)[0] for (mi, *_), p in zip(jobs, params)]
+    for flags in (sd.BATCH_ZERO_MAPS, sd.BATCH_GRAPH | sd.BATCH_ZERO_MAPS):
+        d_maps = [torch.full((p.grid_dim * p.grid_dim,), 9.0, dtype=torch.float64, device="cuda")
+                  for p in params]
+        b = sd.Batch([(cutouts[mi], p, d.data_ptr()) for (mi, *_), p, d in
+                      zip(jobs, params, d_maps)], flags)
+        for _ in range(2):
+            b.launch()
+            b.sync()
+            for k, (d, w) in enumerate(zip(d_maps, want)):
+                assert np.array_equal(d.cpu().numpy().reshape(w.shape), w), (flags, k)
+        b.close()
+
+
 def test_batch_autotune_keeps_results(sd, torch_cuda, cutouts):
     torch = torch_cuda
     params = [_params(sd, G, S, ax, 1, 77 + k) for k, (_, G, S, ax) in enumerate(JOBS)]
