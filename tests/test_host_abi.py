@@ -275,3 +275,94 @@ def test_triangulate_cache_answers_repeated_inputs_without_the_backend():
         L.dtfe_set_triangulation_cache(1024 << 20)
         L.dtfe_set_triangulator.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.dtfe_set_triangulator(None, None)
+
+
+def test_write_rho_and_write_image(tmp_path):
+    """The example driver's writers (src/io.c): write_rho writes the doubles
+    raw; write_image writes a baseline palette TIFF of log(rho + 1) scaled to
+    0..128 between the smallest positive and the largest value, and nothing
+    for negative or NaN maps."""
+    import struct
+
+    from sdtfe_b200 import lib
+
+    L = lib()
+    L.write_rho.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
+    L.write_rho.restype = ctypes.c_int
+    L.write_image.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int]
+    L.write_image.restype = None
+    G = 5
+    rho = np.zeros(G * G)
+    rho[3:] = np.geomspace(0.5, 900.0, G * G - 3)
+    rho[7] = 0.0
+    p = ctypes.c_void_p(rho.ctypes.data)
+    fn = str(tmp_path / "m.rho.bin").encode()
+    assert L.write_rho(fn, ctypes.byref(p), G * G) == G * G
+    assert np.array_equal(np.fromfile(fn.decode(), np.float64), rho)
+
+    img = str(tmp_path / "m.rho.tiff").encode()
+    L.write_image(img, rho.ctypes.data, G)
+    b = open(img.decode(), "rb").read()
+    assert b[:4] == b"II*\x00"
+    ifd = struct.unpack_from("<I", b, 4)[0]
+    n = struct.unpack_from("<H", b, ifd)[0]
+    tags = {}
+    for k in range(n):
+        tag, typ, cnt, val = struct.unpack_from("<HHII", b, ifd + 2 + 12 * k)
+        tags[tag] = (typ, cnt, val if typ == 4 or cnt > 1 else val & 0xFFFF)
+    assert tags[256][2] == G and tags[257][2] == G and tags[258][2] == 8
+    assert tags[259][2] == 1 and tags[262][2] == 3 and tags[277][2] == 1
+    off, count = tags[273][2], tags[279][2]
+    assert count == G * G
+    pix = np.frombuffer(b, np.uint8, count, off)
+    pos = rho > 0
+    lo, hi = np.log(rho[pos].min() + 1.0), np.log(rho.max() + 1.0)
+    want = np.zeros(G * G, np.uint8)
+    want[pos] = (128.0 * (np.log(rho[pos] + 1.0) - lo) / (hi - lo)).astype(np.uint8)
+    assert np.array_equal(pix, want)
+    cmap = np.frombuffer(b, "<u2", 768, tags[320][2])
+    x = np.arange(256) / 255.0
+    for c, chan in zip((3.0, 2.0, 1.0), cmap.reshape(3, 256)):
+        ref = np.floor(np.clip(1.5 - np.abs(4 * x - c), 0, 1) * 65535 + 0.5)
+        assert np.array_equal(chan, ref.astype(np.uint16))
+
+    for bad in (-1.0, np.nan):
+        r2 = rho.copy()
+        r2[4] = bad
+        f2 = str(tmp_path / "bad.tiff").encode()
+        L.write_image(f2, r2.ctypes.data, G)
+        assert not (tmp_path / "bad.tiff").exists()
+
+
+def write_positions(path, n, seed=3):
+    """n float32 positions in the example driver's layout (x[n], y[n], z[n]),
+    a Gaussian blob about the unit box's centre."""
+    p = np.random.default_rng(seed).normal(0.5, 0.08, (n, 3)).astype(np.float32)
+    np.ascontiguousarray(p.T).tofile(path)
+
+
+def run_cli(tmp_path, n=3000, G=32, seed="7"):
+    import os
+    import subprocess
+
+    write_positions(tmp_path / "pts.bin", n)
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "sdtfe_b200",
+                       "dtfe")
+    env = dict(os.environ, SDTFE_SEED=seed)
+    return subprocess.run([exe, "pts.bin", str(n), str(G), "0.5", "0.5", "0.5", "1", "1", "1",
+                           "0", "4", "1"], cwd=tmp_path, env=env, capture_output=True, text=True,
+                          timeout=300)
+
+
+def test_cli_triangulates_through_the_registered_qhull(tmp_path):
+    """The dtfe program reads the reference driver's arguments and file
+    layout, and triangulates through the SciPy Qhull it registers (the map
+    itself needs the GPU: without one the program stops there with an
+    error)."""
+    import torch
+
+    r = run_cli(tmp_path)
+    assert "Using prng seed: 7" in r.stdout
+    assert "Done creating" in r.stdout, r.stdout + r.stderr
+    if not torch.cuda.is_available():
+        assert r.returncode != 0 and "compute_density failed" in r.stderr
