@@ -146,7 +146,16 @@ class QhullPool:
     def __init__(self, tasks):
         import multiprocessing as mp
 
-        self.procs = max(1, min(len(tasks), len(os.sched_getaffinity(0)), 32))
+        # one worker per core, as memory allows: Qhull takes about 3 GB per
+        # million points, and the largest tasks (up to 9.2M points) run first
+        try:
+            import psutil
+
+            avail_gb = psutil.virtual_memory().available / 2**30
+        except ImportError:
+            avail_gb = 256.0
+        by_mem = max(1, int((avail_gb - 40.0) // 8.0))
+        self.procs = max(1, min(len(tasks), len(os.sched_getaffinity(0)), 32, by_mem))
         order = tasks[:1] + sorted(tasks[1:], key=lambda t: -t[2])
         self.t0 = time.perf_counter()
         self.pool = mp.get_context("spawn").Pool(self.procs)
@@ -650,13 +659,18 @@ def section_large_field(args, sd, torch, dev, stream, flush, tri):
     grid (supersampling 1, the reference's column walk), mixed against FP64:
     device time, crossings, max/RMS relative error, projected mass."""
     pos4, tetra, t_q = tri.get("large", 0)
-    mesh = sd.Mesh(pos4, tetra, 1.0, sd.MESH_LAZY)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mesh = sd.Mesh(pos4, tetra, 1.0, sd.MESH_LAZY)  # upload, densities (CSR), gradients
+    t_build = time.perf_counter() - t0
     tri.drop("large", 0)
     info = mesh.info()
     sptr = stream.cuda_stream
     out = {"workload": "192^3 lattice (sigma 0.3 spacing) + 30% in 2000 r^-2 clusters (r 0.01), "
                        "float32; 8192^2 x 4 map and 512^3 grid (ss 1), mixed vs FP64",
-           "particles": int(len(pos4)), "tets": int(info.n_tetra), "qhull_host_s": round(t_q, 1)}
+           "particles": int(len(pos4)), "tets": int(info.n_tetra), "qhull_host_s": round(t_q, 1),
+           "mesh_create_s": round(t_build, 3),
+           "adjacency_max": int(mesh.adjacency().max())}
     G, S = 8192, 4
     kw = dict(grid_dim=G, box_len=1.0, box_len_z=1.0, center=(0.5, 0.5, 0.5), n_samples=S,
               seed=909)
