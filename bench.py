@@ -207,6 +207,12 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # a short timed region may end before the first 200 ms sample:
+            # start timing once nvidia-smi is reporting (at most 2 s)
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 2.0:
+                time.sleep(0.01)
+            self.first = len(self.lines)  # samples from here on fall in the timed region
         except FileNotFoundError:
             self.proc = None
 
@@ -224,7 +230,8 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines[getattr(self, "first", 0):] or self.lines[-1:]
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
