@@ -704,7 +704,7 @@ def section_large_field(args, sd, torch, dev, stream, flush, tri):
                   "fp64_fallbacks": s32.fp64_fallbacks,
                   "max_rel_err": e_max, "rms_rel_err": e_rms,
                   "mass_rel_diff": float(a32.sum() / G / G / len(pos4) - 1.0),
-                  "hull_triangles": int(info.n_hull_tri[0]) if info.n_hull_tri[0] >= 0 else None}
+                  "hull_triangles": int(mesh.info().n_hull_tri[0])}
     del d_map, res
     torch.cuda.empty_cache()
     GG = 512

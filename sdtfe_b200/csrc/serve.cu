@@ -4,7 +4,8 @@
 // One host thread runs the loop.  Each pass it
 //   1. retires finished iterations and starts the device->host copy of every
 //      request whose tiles have all been walked,
-//   2. completes requests whose copies have landed,
+//   2. completes requests whose copies have landed (maps for pageable host
+//      memory are copied by a second thread, so the loop never waits on them),
 //   3. admits queued requests while a slot is free and the request's map plus
 //      any walk records it still needs fit the device budget (records of idle
 //      (mesh, axis) pairs are evicted least recently used first; a request
@@ -49,7 +50,7 @@ struct Request {
   MapGeom g{};
   size_t map_bytes = 0;
   double* d_map = nullptr;
-  double* staging = nullptr;   // pinned copy target when host_map is pageable
+  bool pageable = false;       // host_map is not pinned: the copier thread copies it
   int stat_slot = -1;
   long long tiles = 0, next_tile = 0;
   double rays_per_tile = 1;
@@ -92,7 +93,6 @@ struct dtfe_server_s {
   std::vector<Request*> active;  // admission order
   std::unordered_map<uint64_t, Request*> requests;
   std::map<std::pair<int, int>, Resident> resident;
-  std::multimap<size_t, double*> staging_free;
   std::vector<int> free_stat_slots;
   size_t in_use = 0, peak = 0;
   uint64_t next_id = 1;
@@ -100,6 +100,14 @@ struct dtfe_server_s {
   bool stop = false;
   dtfe_status_t fatal = DTFE_OK;
   std::thread thread;
+  // requests whose map goes to the caller's pageable memory: copied by this
+  // thread on its own stream (a pageable copy blocks the thread that issues
+  // it), so that the loop keeps launching while large maps are copied out
+  std::thread copier;
+  cudaStream_t copy_out = nullptr;
+  std::deque<Request*> copy_q;
+  std::condition_variable cv_copy;
+  bool copier_stop = false;
   cudaStream_t setup = nullptr, copy = nullptr, streams[2] = {nullptr, nullptr};
   cudaEvent_t ev_setup = nullptr;
   cudaMemPool_t pool = nullptr;
@@ -164,10 +172,6 @@ void release(Server* S, Request* r) {
     S->in_use -= r->map_bytes;
     r->d_map = nullptr;
   }
-  if (r->staging) {
-    S->staging_free.emplace(r->map_bytes, r->staging);
-    r->staging = nullptr;
-  }
   if (r->stat_slot >= 0) {
     S->free_stat_slots.push_back(r->stat_slot);
     r->stat_slot = -1;
@@ -218,15 +222,7 @@ dtfe_status_t admit_one(Server* S, Request* r) {
   const bool pinned = cudaPointerGetAttributes(&pa, r->host_map) == cudaSuccess &&
                       pa.type == cudaMemoryTypeHost;
   cudaGetLastError();  // a pageable pointer may leave an error behind on old drivers
-  if (!pinned) {
-    auto it = S->staging_free.find(r->map_bytes);
-    if (it != S->staging_free.end()) {
-      r->staging = it->second;
-      S->staging_free.erase(it);
-    } else {
-      SDTFE_CUDA(cudaMallocHost(reinterpret_cast<void**>(&r->staging), r->map_bytes));
-    }
-  }
+  r->pageable = !pinned;
   SDTFE_CUDA(cudaEventCreateWithFlags(&r->ev_copy, cudaEventDisableTiming));
   r->tiles = r->p.precision == DTFE_MIXED ? map_tiles32(r->g, S->cfg.variant) : map_tiles64(r->g);
   r->rays_per_tile = (double)r->p.grid_dim * r->p.grid_dim * r->p.n_samples / (double)r->tiles;
@@ -410,8 +406,13 @@ bool launch_next(Server* S) {
 }
 
 void start_copy(Server* S, Request* r) {
-  double* dst = r->staging ? r->staging : r->host_map;
-  cudaError_t e = cudaMemcpyAsync(dst, r->d_map, r->map_bytes, cudaMemcpyDeviceToHost, S->copy);
+  if (r->pageable) {  // every iteration holding its tiles has finished: the map is ready
+    S->copy_q.push_back(r);
+    S->cv_copy.notify_one();
+    return;
+  }
+  cudaError_t e = cudaMemcpyAsync(r->host_map, r->d_map, r->map_bytes, cudaMemcpyDeviceToHost,
+                                  S->copy);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(S->h_stats + (size_t)r->stat_slot * kStatCount,
                         S->d_stats + (size_t)r->stat_slot * kStatCount,
@@ -454,36 +455,66 @@ bool retire(Server* S) {
   return progress;
 }
 
-bool finish_copies(Server* S, std::unique_lock<std::mutex>& lk) {
+// with S->mu held: the request's counters and latency, then its resources
+void complete(Server* S, Request* r) {
+  const unsigned long long* c = S->h_stats + (size_t)r->stat_slot * kStatCount;
+  dtfe_map_stats_t& s = r->info.stats;
+  memset(&s, 0, sizeof(s));
+  s.rays = c[kStatRays];
+  s.visits = c[kStatVisits];
+  for (int k = 0; k < DTFE_N_RAY_STATUS; ++k) s.status[k] = c[kStatStatus0 + k];
+  s.fp64_fallbacks = c[kStatFallback];
+  r->info.iterations = r->iterations;
+  r->info.latency_ms = ms_between(r->t_submit, Clock::now());
+  r->info.status = DTFE_OK;
+  release(S, r);
+  r->done = true;
+  ++S->st.completed;
+  S->st.rays += s.rays;
+  S->st.visits += s.visits;
+}
+
+bool finish_copies(Server* S) {
   std::vector<Request*> landed;
   for (Request* r : S->active)
     if (r->copying && cudaEventQuery(r->ev_copy) == cudaSuccess) landed.push_back(r);
   if (landed.empty()) return false;
   for (Request* r : landed) {
-    if (r->staging) {  // the caller's pageable buffer: copy without holding the lock
-      lk.unlock();
-      memcpy(r->host_map, r->staging, r->map_bytes);
-      lk.lock();
-    }
-    const unsigned long long* c = S->h_stats + (size_t)r->stat_slot * kStatCount;
-    dtfe_map_stats_t& s = r->info.stats;
-    memset(&s, 0, sizeof(s));
-    s.rays = c[kStatRays];
-    s.visits = c[kStatVisits];
-    for (int k = 0; k < DTFE_N_RAY_STATUS; ++k) s.status[k] = c[kStatStatus0 + k];
-    s.fp64_fallbacks = c[kStatFallback];
-    r->info.iterations = r->iterations;
-    r->info.latency_ms = ms_between(r->t_submit, Clock::now());
-    r->info.status = DTFE_OK;
     r->copying = false;
-    release(S, r);
-    r->done = true;
-    ++S->st.completed;
-    S->st.rays += s.rays;
-    S->st.visits += s.visits;
+    complete(S, r);
   }
   S->cv_done.notify_all();
   return true;
+}
+
+void copy_out_loop(Server* S) {
+  cudaSetDevice(S->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  for (;;) {
+    S->cv_copy.wait(lk, [&] { return S->copier_stop || !S->copy_q.empty(); });
+    if (S->copy_q.empty()) return;  // stopping, nothing left
+    Request* r = S->copy_q.front();
+    S->copy_q.pop_front();
+    unsigned long long* h = S->h_stats + (size_t)r->stat_slot * kStatCount;
+    const unsigned long long* d = S->d_stats + (size_t)r->stat_slot * kStatCount;
+    lk.unlock();
+    cudaError_t e = cudaMemcpyAsync(r->host_map, r->d_map, r->map_bytes, cudaMemcpyDeviceToHost,
+                                    S->copy_out);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h, d, sizeof(unsigned long long) * kStatCount, cudaMemcpyDeviceToHost,
+                          S->copy_out);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->copy_out);
+    lk.lock();
+    if (e == cudaSuccess) {
+      complete(S, r);
+    } else {
+      set_error(DTFE_ERR_CUDA, "result copy: %s", cudaGetErrorString(e));
+      release(S, r);
+      fail_request(S, r, DTFE_ERR_CUDA);
+    }
+    S->cv_done.notify_all();
+    S->cv_work.notify_one();  // the loop may be waiting for the memory this freed
+  }
 }
 
 void loop(Server* S) {
@@ -491,7 +522,7 @@ void loop(Server* S) {
   std::unique_lock<std::mutex> lk(S->mu);
   for (;;) {
     bool progress = retire(S);
-    progress |= finish_copies(S, lk);
+    progress |= finish_copies(S);
     progress |= admit(S);
     progress |= launch_next(S);
     bool busy = !S->active.empty();
@@ -505,17 +536,15 @@ void loop(Server* S) {
 }
 
 void free_server(Server* S) {
-  for (cudaStream_t s : {S->setup, S->copy, S->streams[0], S->streams[1]})
+  for (cudaStream_t s : {S->setup, S->copy, S->copy_out, S->streams[0], S->streams[1]})
     if (s) cudaStreamSynchronize(s);
   for (auto& kv : S->requests) {
     Request* r = kv.second;
     if (r->d_map) cudaFreeAsync(r->d_map, S->copy);
-    if (r->staging) cudaFreeHost(r->staging);
     if (r->ev_copy) cudaEventDestroy(r->ev_copy);
     delete r;
   }
   if (S->copy) cudaStreamSynchronize(S->copy);
-  for (auto& kv : S->staging_free) cudaFreeHost(kv.second);
   for (Slot& sl : S->slot) {
     if (sl.ev) cudaEventDestroy(sl.ev);
     if (sl.h_jobs) cudaFreeHost(sl.h_jobs);
@@ -526,7 +555,7 @@ void free_server(Server* S) {
   if (S->d_stats) cudaFree(S->d_stats);
   if (S->h_stats) cudaFreeHost(S->h_stats);
   if (S->ev_setup) cudaEventDestroy(S->ev_setup);
-  for (cudaStream_t s : {S->setup, S->copy, S->streams[0], S->streams[1]})
+  for (cudaStream_t s : {S->setup, S->copy, S->copy_out, S->streams[0], S->streams[1]})
     if (s) cudaStreamDestroy(s);
   if (S->pool) cudaMemPoolDestroy(S->pool);
   delete S;
@@ -575,7 +604,7 @@ dtfe_status_t dtfe_server_create(const dtfe_server_config_t* cfg, dtfe_server_t*
     S->auto_budget = true;
     st = set_auto_budget(S);
   }
-  for (cudaStream_t* s : {&S->setup, &S->copy, &S->streams[0], &S->streams[1]})
+  for (cudaStream_t* s : {&S->setup, &S->copy, &S->copy_out, &S->streams[0], &S->streams[1]})
     if (st == DTFE_OK) cuda(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking), "stream");
   if (st == DTFE_OK) cuda(cudaEventCreateWithFlags(&S->ev_setup, cudaEventDisableTiming), "event");
   for (Slot& sl : S->slot) {
@@ -603,10 +632,19 @@ dtfe_status_t dtfe_server_create(const dtfe_server_config_t* cfg, dtfe_server_t*
   for (int k = S->cfg.max_active - 1; k >= 0; --k) S->free_stat_slots.push_back(k);
   S->st.budget = S->cfg.device_budget;
   try {
+    S->copier = std::thread(copy_out_loop, S);
     S->thread = std::thread(loop, S);
   } catch (...) {
+    if (S->copier.joinable()) {
+      {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->copier_stop = true;
+      }
+      S->cv_copy.notify_all();
+      S->copier.join();
+    }
     free_server(S);
-    return set_error(DTFE_ERR_NOMEM, "could not start the serving thread");
+    return set_error(DTFE_ERR_NOMEM, "could not start the serving threads");
   }
   *out = S;
   return DTFE_OK;
@@ -722,7 +760,13 @@ dtfe_status_t dtfe_server_destroy(dtfe_server_t S) {
     S->stop = true;
   }
   S->cv_work.notify_all();
-  if (S->thread.joinable()) S->thread.join();
+  if (S->thread.joinable()) S->thread.join();  // returns once nothing is active
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->copier_stop = true;
+  }
+  S->cv_copy.notify_all();
+  if (S->copier.joinable()) S->copier.join();
   free_server(S);
   return DTFE_OK;
 }
