@@ -59,6 +59,8 @@ struct Request {
   bool holds_records = false;  // counted in its (mesh, axis) records' references
   bool copying = false, done = false;
   cudaEvent_t ev_copy = nullptr;
+  cudaEvent_t ev_ready = nullptr;  // its records, map and counters are set up
+  bool ready = false;              // ev_ready has been seen complete
   dtfe_request_info_t info{};
 };
 
@@ -185,6 +187,10 @@ void release(Server* S, Request* r) {
     cudaEventDestroy(r->ev_copy);
     r->ev_copy = nullptr;
   }
+  if (r->ev_ready) {
+    cudaEventDestroy(r->ev_ready);
+    r->ev_ready = nullptr;
+  }
   S->active.erase(std::remove(S->active.begin(), S->active.end(), r), S->active.end());
 }
 
@@ -215,8 +221,11 @@ dtfe_status_t admit_one(Server* S, Request* r) {
   S->free_stat_slots.pop_back();
   SDTFE_CUDA(cudaMemsetAsync(S->d_stats + (size_t)r->stat_slot * kStatCount, 0,
                              sizeof(unsigned long long) * kStatCount, S->setup));
-  SDTFE_CUDA(cudaEventRecord(S->ev_setup, S->setup));
-  for (cudaStream_t s : S->streams) SDTFE_CUDA(cudaStreamWaitEvent(s, S->ev_setup, 0));
+  // only the iterations that walk this request's tiles wait for its set-up
+  // (launch_iteration); the others keep the GPU busy meanwhile
+  SDTFE_CUDA(cudaEventCreateWithFlags(&r->ev_ready, cudaEventDisableTiming));
+  SDTFE_CUDA(cudaEventRecord(r->ev_ready, S->setup));
+  r->ready = false;
   // pinned caller buffers take the copy directly
   cudaPointerAttributes pa{};
   const bool pinned = cudaPointerGetAttributes(&pa, r->host_map) == cudaSuccess &&
@@ -276,9 +285,16 @@ bool admit(Server* S) {
 
 // tiles of each request for the next iteration
 void share_tiles(Server* S, std::vector<std::pair<Request*, long long>>* out) {
-  std::vector<Request*> rs;
-  for (Request* r : S->active)
-    if (r->next_tile < r->tiles) rs.push_back(r);
+  // requests whose set-up (record build, map clearing) has finished first; the
+  // others only when no ready request has tiles left, so that a record build
+  // does not hold up the requests already running
+  std::vector<Request*> rs, waiting;
+  for (Request* r : S->active) {
+    if (r->next_tile >= r->tiles) continue;
+    if (!r->ready && r->ev_ready && cudaEventQuery(r->ev_ready) == cudaSuccess) r->ready = true;
+    (r->ready ? rs : waiting).push_back(r);
+  }
+  if (rs.empty()) rs.swap(waiting);
   if (rs.empty()) return;
   auto rest = [](const Request* r) { return (double)(r->tiles - r->next_tile) * r->rays_per_tile; };
   // The iteration's rays: quantum_rays under light load (short iterations, so
@@ -309,6 +325,7 @@ dtfe_status_t launch_iteration(Server* S, Slot& sl, const std::vector<std::pair<
   std::vector<BatchMap> maps[2];  // mixed, FP64
   for (const auto& rt : take) {
     Request* r = rt.first;
+    if (!r->ready) SDTFE_CUDA(cudaStreamWaitEvent(s, r->ev_ready, 0));
     BatchMap b;
     b.mesh = &S->meshes[r->mesh_id]->m;
     b.g = r->g;
@@ -542,6 +559,7 @@ void free_server(Server* S) {
     Request* r = kv.second;
     if (r->d_map) cudaFreeAsync(r->d_map, S->copy);
     if (r->ev_copy) cudaEventDestroy(r->ev_copy);
+    if (r->ev_ready) cudaEventDestroy(r->ev_ready);
     delete r;
   }
   if (S->copy) cudaStreamSynchronize(S->copy);
