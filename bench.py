@@ -75,7 +75,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--sections", default="batch,serving,large_field",
+    ap.add_argument("--sections", default="plain_small,batch,serving,large_field",
                     help="extra sections on one GPU: batch (64 cutouts in one persistent launch), "
                          "serving (request stream with continuous batching); 'none' to skip")
     ap.add_argument("--serve-handles", type=int, default=256)
@@ -443,6 +443,8 @@ def plan_sections(args):
         tasks += [("clustered", i, n, seed) for i, (n, seed) in enumerate(serving_cutouts(args))]
     if "large_field" in sections:
         tasks += [("large", 0, 9_201_254, 5)]
+    if "plain_small" in sections and args.workload != "uniform":
+        tasks += [("main", "uniform", 32768, 0)]
     return QhullPool(tasks), sections
 
 
@@ -657,6 +659,59 @@ def section_serving(args, sd, torch, tri):
                                       out["capacity_fp64"]["rays_per_s"])
     for m in meshes:
         m.close()
+    return out
+
+
+def section_plain_small(args, sd, torch, dev, stream, flush, tri):
+    """The plain method at its own, CPU-runnable size: 32,768 uniform float64
+    points, a 256^2 map with 4 samples per pixel, FP64 throughout (and the
+    mixed path beside it), against the reference's own compute_density over
+    the whole map on every host core - no window, no extrapolation."""
+    pos4, tetra, t_q = tri.get("main", "uniform")
+    spec = workload("uniform")[2]
+    mesh = sd.Mesh(pos4, tetra, 1.0)
+    sptr = stream.cuda_stream
+    d_map = torch.zeros(spec.grid_dim ** 2, dtype=torch.float64, device=dev)
+    out = {"workload": "uniform_32k_256x4 (32,768 uniform float64 points, 256^2 x 4, FP64)",
+           "particles": len(pos4), "tets": len(tetra), "rays": spec.rays}
+    maps = {}
+    for name, prec in (("fp64", sd.DTFE_FP64), ("mixed", sd.DTFE_MIXED)):
+        p = sd.map_params(spec.grid_dim, spec.box_len, spec.box_len_z, spec.center,
+                          spec.n_samples, 0.0, 4242, precision=prec)
+
+        def one(p=p):
+            d_map.zero_()
+            mesh.map_device(p, d_map.data_ptr(), sptr)
+        one()
+        ms = float(np.median(timed_launches(torch, stream, flush, one, max(args.steps, 3))))
+        st = mesh.last_stats()
+        maps[name] = d_map.cpu().numpy().copy()
+        out[name] = {"ms_per_map": ms, "rays_per_s": spec.rays / (ms / 1e3),
+                     "visits_per_ray": st.visits / spec.rays}
+    e_max, e_rms = max_rel(maps["mixed"], maps["fp64"])
+    out["mixed"].update(max_rel_err=e_max, rms_rel_err=e_rms,
+                        speedup_over_fp64=out["fp64"]["ms_per_map"] / out["mixed"]["ms_per_map"])
+    out["fp64"]["mass_rel_diff"] = float(maps["fp64"].sum() / spec.grid_dim ** 2 / len(pos4) - 1)
+    mesh.close()
+    try:  # the reference's compute_density, whole map, all host cores
+        ref = RefCPU()
+        rho = np.zeros(spec.grid_dim ** 2)
+        ts = []
+        for _ in range(3):
+            rho[:] = 0.0
+            pd = pos4.copy()
+            t = time.perf_counter()
+            ref._quiet(lambda: ref.R.compute_density(pd, tetra, spec.grid_dim, spec.box_len,
+                                                     spec.box_len_z, rho, 1.0, spec.center,
+                                                     spec.n_samples, 0.0))
+            ts.append(time.perf_counter() - t)
+        t = float(np.median(ts))
+        out["reference_cpu"] = {"s_per_map": t, "rays_per_s": spec.rays / t, "cores": ref.cores,
+                                "mass_rel_diff": float(rho.sum() / spec.grid_dim ** 2 /
+                                                       len(pos4) - 1)}
+        out["fp64"]["speedup_over_reference_cpu"] = t / (out["fp64"]["ms_per_map"] / 1e3)
+    except Exception as e:
+        out["reference_cpu"] = {"unavailable": f"{type(e).__name__}: {e}"}
     return out
 
 
@@ -917,6 +972,8 @@ def run_ours(args, pre=None):
             cpu = {"value": None, "unit": "rays/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {e}"}
 
+    run_section("plain_small",
+                lambda: section_plain_small(args, sd, torch, dev, stream, flush, tri))
     run_section("serving", lambda: section_serving(args, sd, torch, tri))
     run_section("large_field",
                 lambda: section_large_field(args, sd, torch, dev, stream, flush, tri))
