@@ -551,15 +551,22 @@ __device__ __forceinline__ bool fast_step(const MixConf& C, const RayState& r, i
                        ~(unsigned)nb.w) >> 31 &
                       (k0 | k1 | k2) & (umin > bound ? 1u : 0u);
   if (!ok) return false;
-  const int k = (int)(k1 | (k2 << 1));
-  const int next = sel3(k, nb.x, nb.y, nb.z);
+  // The exit slot k is one-hot in (k0, k1, k2) (exactly one is set once ok
+  // holds); every choice below picks by those bits with masks, so that lanes
+  // leaving through different faces stay on one instruction stream.
+  const unsigned m0 = 0u - k0, m1 = 0u - k1, m2 = 0u - k2;
+  const auto pick = [m0, m1, m2](float a, float b, float c) {
+    return __uint_as_float((__float_as_uint(a) & m0) | (__float_as_uint(b) & m1) |
+                           (__float_as_uint(c) & m2));
+  };
+  const int next = (int)(((unsigned)nb.x & m0) | ((unsigned)nb.y & m1) | ((unsigned)nb.z & m2));
   if (next < -1) return false;  // a neighbour that does not list this tet
   // exit face: apex (slot 3) and slots i = k+1, j = k+2 (mod 3); the weight of
   // each corner is the product of the face edge opposite it
-  const float w3 = sel3(k, e12, e20, e01);
-  const float wi = -sel3(k, a2, a0, a1);
-  const float wj = sel3(k, a1, a2, a0);
-  const float zi = sel3(k, z.y, z.z, z.x), zj = sel3(k, z.z, z.x, z.y);
+  const float w3 = pick(e12, e20, e01);
+  const float wi = -pick(a2, a0, a1);
+  const float wj = pick(a1, a2, a0);
+  const float zi = pick(z.y, z.z, z.x), zj = pick(z.z, z.x, z.y);
   const float den = w3 + wi + wj;
   const float rr = __fdividef(1.f, den);
   const float cond = 3.f * bound * fabsf(rr);  // relative error of the weights
