@@ -93,12 +93,14 @@ typedef struct {
 } dtfe_mesh_info_t;
 
 /* One mixed-map kernel variant: threads per block, blocks per SM the register
- * budget allows, and the pixel tile shape (0: square-ish, 1: row strip). */
+ * budget allows, the pixel tile shape (0: square-ish, 1: row strip), and the
+ * rays each thread walks per tile. */
 typedef struct {
   int block;
   int min_blocks;
   int wide_tile;
   double ms;             /* autotuner timing on its window (0 if not timed)     */
+  int rays_per_thread;   /* rays each thread walks per tile                      */
 } dtfe_variant_t;
 
 /* mesh flags */

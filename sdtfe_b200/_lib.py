@@ -67,7 +67,8 @@ class MeshInfo(ctypes.Structure):
 
 
 class Variant(ctypes.Structure):
-    _fields_ = [("block", _i), ("min_blocks", _i), ("wide_tile", _i), ("ms", _d)]
+    _fields_ = [("block", _i), ("min_blocks", _i), ("wide_tile", _i), ("ms", _d),
+                ("rays_per_thread", _i)]
 
 
 class BatchJob(ctypes.Structure):
@@ -336,7 +337,7 @@ class Mesh:
         best = _i()
         _check(lib().dtfe_autotune(self.h, ctypes.byref(params), ctypes.byref(best), arr))
         return best.value, [dict(block=v.block, min_blocks=v.min_blocks, wide_tile=v.wide_tile,
-                                 ms=v.ms) for v in arr]
+                                 rays_per_thread=v.rays_per_thread, ms=v.ms) for v in arr]
 
     def set_variant(self, variant: int):
         _check(lib().dtfe_set_variant(self.h, variant))
@@ -407,7 +408,7 @@ class Batch:
         best = _i()
         _check(lib().dtfe_batch_autotune(self.h, ctypes.byref(best), arr))
         return best.value, [dict(block=v.block, min_blocks=v.min_blocks, wide_tile=v.wide_tile,
-                                 ms=v.ms) for v in arr]
+                                 rays_per_thread=v.rays_per_thread, ms=v.ms) for v in arr]
 
     def set_variant(self, v: int):
         _check(lib().dtfe_batch_set_variant(self.h, v))

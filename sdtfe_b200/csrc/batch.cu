@@ -277,7 +277,8 @@ dtfe_status_t dtfe_batch_autotune(dtfe_batch_t b, int* best, dtfe_variant_t* tim
       ms_v = ms;
     }
     if (timings) {
-      map32_variant_info(v, &timings[v].block, &timings[v].min_blocks, &timings[v].wide_tile);
+      map32_variant_info(v, &timings[v].block, &timings[v].min_blocks, &timings[v].wide_tile,
+                         &timings[v].rays_per_thread);
       timings[v].ms = ms_v;
     }
     if (st == DTFE_OK && (best_v < 0 || ms_v < best_ms)) {

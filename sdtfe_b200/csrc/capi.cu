@@ -302,7 +302,8 @@ dtfe_status_t dtfe_autotune(dtfe_mesh_t h, const dtfe_map_params_t* p, int* best
       if (rep == 1 || (rep == 2 && ms < ms_v)) ms_v = ms;
     }
     if (timings) {
-      map32_variant_info(v, &timings[v].block, &timings[v].min_blocks, &timings[v].wide_tile);
+      map32_variant_info(v, &timings[v].block, &timings[v].min_blocks, &timings[v].wide_tile,
+                         &timings[v].rays_per_thread);
       timings[v].ms = ms_v;
     }
     if (st == DTFE_OK && (best_v < 0 || ms_v < best_ms)) {

@@ -147,7 +147,7 @@ dtfe_status_t launch_trace32(Mesh& m, int axis, int n_rays, const double* d_x, c
                              double* d_rho, int* d_crossed, int* d_status, int* d_visits,
                              int max_record, cudaStream_t s);
 int num_map32_variants();
-void map32_variant_info(int i, int* block, int* minb, int* wide);
+void map32_variant_info(int i, int* block, int* minb, int* wide, int* rpt);
 dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
                             uint64_t seed, int max_visits, double* d_grid, cudaStream_t s);
 dtfe_status_t launch_grid32(Mesh& m, int G, double box_len, const double center[3], unsigned ss,

@@ -1269,16 +1269,24 @@ void tile_shape32(int threads, int S, int wide, int* TW, int* TH) {
 static_assert(sizeof(int2) == kLocBytes, "tile location layout");
 typedef void (*MapKernel32)(const MapArgs32, const int2*);
 
+// A kernel instantiation, its pixel-tile shape, and the rays each thread
+// walks per tile (rpt): with rpt > 1 a tile holds rpt x block rays, and a
+// lane that finishes a ray early starts its next one while the others walk,
+// so the warp's ray-length tail and the end-of-tile barrier are paid once per
+// rpt rays.
 struct Variant32 {
   MapKernel32 kernel;
-  int block, minb, wide;
+  int block, minb, wide, rpt;
 };
 
 const Variant32 kVariants32[] = {
-    {k_map32<256, 2>, 256, 2, 0}, {k_map32<256, 3>, 256, 3, 0}, {k_map32<256, 4>, 256, 4, 0},
-    {k_map32<128, 4>, 128, 4, 0}, {k_map32<128, 6>, 128, 6, 0}, {k_map32<256, 2>, 256, 2, 1},
-    {k_map32<256, 3>, 256, 3, 1}, {k_map32<128, 8>, 128, 8, 0}, {k_map32<64, 16>, 64, 16, 0},
-    {k_map32<32, 32>, 32, 32, 0},
+    {k_map32<256, 2>, 256, 2, 0, 1}, {k_map32<256, 3>, 256, 3, 0, 1},
+    {k_map32<256, 4>, 256, 4, 0, 1}, {k_map32<128, 4>, 128, 4, 0, 1},
+    {k_map32<128, 6>, 128, 6, 0, 1}, {k_map32<256, 2>, 256, 2, 1, 1},
+    {k_map32<256, 3>, 256, 3, 1, 1}, {k_map32<128, 8>, 128, 8, 0, 1},
+    {k_map32<64, 16>, 64, 16, 0, 1}, {k_map32<32, 32>, 32, 32, 0, 1},
+    {k_map32<128, 8>, 128, 8, 0, 2}, {k_map32<64, 16>, 64, 16, 0, 2},
+    {k_map32<32, 32>, 32, 32, 0, 2}, {k_map32<128, 8>, 128, 8, 0, 4},
 };
 constexpr int kNumVariants32 = sizeof(kVariants32) / sizeof(kVariants32[0]);
 constexpr int kDefaultVariant32 = 7;  // (128, 8): the usual winner on B200
@@ -1287,7 +1295,8 @@ typedef void (*BatchKernel32)(const BatchTable32, unsigned long long*, const int
 const BatchKernel32 kBatch32[] = {k_batch32<256, 2>, k_batch32<256, 3>, k_batch32<256, 4>,
                                   k_batch32<128, 4>, k_batch32<128, 6>, k_batch32<256, 2>,
                                   k_batch32<256, 3>, k_batch32<128, 8>, k_batch32<64, 16>,
-                                  k_batch32<32, 32>};
+                                  k_batch32<32, 32>, k_batch32<128, 8>, k_batch32<64, 16>,
+                                  k_batch32<32, 32>, k_batch32<128, 8>};
 static_assert(sizeof(kBatch32) / sizeof(kBatch32[0]) == kNumVariants32, "one batch kernel per variant");
 
 // Checks that an axis has what the mixed walk reads.
@@ -1315,7 +1324,7 @@ dtfe_status_t map_args32(Mesh& m, const MapGeom& g, int vi, double* d_map,
   a.map = d_map;
   a.G = g.G;
   a.S = g.S;
-  tile_shape32(V.block, g.S, V.wide, &a.TW, &a.TH);
+  tile_shape32(V.block * V.rpt, g.S, V.wide, &a.TW, &a.TH);
   a.tiles_x = (g.G + a.TW - 1) / a.TW;
   *tiles_y = (g.G + a.TH - 1) / a.TH;
   a.dxy = g.dxy;
@@ -1431,7 +1440,7 @@ int default_variant32() { return kDefaultVariant32; }
 int map_tiles32(const MapGeom& g, int variant) {
   const Variant32& V = kVariants32[pick_variant32(variant)];
   int TW, TH;
-  tile_shape32(V.block, g.S, V.wide, &TW, &TH);
+  tile_shape32(V.block * V.rpt, g.S, V.wide, &TW, &TH);
   return ((g.G + TW - 1) / TW) * ((g.G + TH - 1) / TH);
 }
 
@@ -1520,9 +1529,10 @@ dtfe_status_t launch_batch32(const BatchPlan& plan, const void* d_jobs, unsigned
 }
 
 int num_map32_variants() { return kNumVariants32; }
-void map32_variant_info(int i, int* block, int* minb, int* wide) {
+void map32_variant_info(int i, int* block, int* minb, int* wide, int* rpt) {
   *block = kVariants32[i].block;
   *minb = kVariants32[i].minb;
   *wide = kVariants32[i].wide;
+  *rpt = kVariants32[i].rpt;
 }
 }  // namespace sdtfe
