@@ -172,3 +172,36 @@ def test_clustered_window_at_single_map_pixel_size(clustered, sd):
     assert np.isin(t64, [sd.RAY_OK, sd.RAY_MISS]).all() and (t64 == sd.RAY_OK).mean() > 0.9
     assert rel_err(g32, g64) <= MIXED_TOL
     assert s32.fp64_fallbacks > 0
+
+
+# --------------------------------------------------------------------------
+# batched-cutouts recipe: a halo at the origin (r^-2 core) in [-1, 1]^3
+# --------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def halo(sd):
+    from sdtfe_b200 import workloads
+
+    pos4 = workloads.halo_cutout(200_000, 3007)
+    m = sd.Mesh(pos4, sd.triangulate(pos4), 1.0)
+    yield m
+    m.close()
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_halo_cutout_mixed_against_fp64(halo, sd, axis):
+    """A 200k-particle halo cutout (the batch configuration's recipe): tets
+    from ~1e-5 in the core to ~0.1 in the background, crossings near z = 0
+    where a large tet meets a small one.  Mixed against FP64 over the whole
+    cutout: the same crossings and statuses, map error <= 1e-5."""
+    kw = dict(grid_dim=256, box_len=2.0, box_len_z=2.0, center=(0.0, 0.0, 0.0), n_samples=8,
+              seed=SEED, axis=axis)
+    g64, s64 = halo.map(sd.map_params(**kw))
+    g32, s32 = halo.map(sd.map_params(**kw, precision=sd.DTFE_MIXED))
+    assert s32.visits == s64.visits and list(s32.status) == list(s64.status)
+    assert rel_err(g32, g64) <= MIXED_TOL
+    # and a 128^2 window on the core at 1/4096 of the box per pixel
+    kw.update(grid_dim=128, box_len=2.0 / 32)
+    g64, s64 = halo.map(sd.map_params(**kw))
+    g32, s32 = halo.map(sd.map_params(**kw, precision=sd.DTFE_MIXED))
+    assert s32.visits == s64.visits
+    assert rel_err(g32, g64) <= MIXED_TOL
