@@ -748,6 +748,19 @@ def section_large_field(args, sd, torch, dev, stream, flush, tri):
         ms = timed_launches(torch, stream, flush, one, reps)
         st = mesh.last_stats()
         res[name] = (float(np.median(ms)), st, d_map.cpu().numpy())
+    # FP64 again with one shared location walk per pixel tile: the large
+    # projected hull is where the reference's per-ray walk from triangle 0
+    # costs the most
+    mesh.set_location(sd.LOCATE_TILE)
+    p = sd.map_params(**kw, precision=sd.DTFE_FP64)
+
+    def one_tile(p=p):
+        d_map.zero_()
+        mesh.map_device(p, d_map.data_ptr(), sptr)
+    ms_tile = float(np.median(timed_launches(torch, stream, flush, one_tile, 1)))
+    st_tile = mesh.last_stats()
+    tile_equal = bool(np.array_equal(d_map.cpu().numpy(), res["fp64"][2]))
+    mesh.set_location(sd.LOCATE_PER_RAY)
     rays = G * G * S
     (m32, s32, a32), (m64, s64, a64) = res["mixed"], res["fp64"]
     e_max, e_rms = max_rel(a32, a64)
@@ -759,7 +772,12 @@ def section_large_field(args, sd, torch, dev, stream, flush, tri):
                   "fp64_fallbacks": s32.fp64_fallbacks,
                   "max_rel_err": e_max, "rms_rel_err": e_rms,
                   "mass_rel_diff": float(a32.sum() / G / G / len(pos4) - 1.0),
-                  "hull_triangles": int(mesh.info().n_hull_tri[0])}
+                  "hull_triangles": int(mesh.info().n_hull_tri[0]),
+                  "fp64_tile_location": {
+                      "ms": ms_tile, "rays_per_s": rays / (ms_tile / 1e3),
+                      "speedup_mixed_over_it": ms_tile / m32, "map_equal": tile_equal,
+                      "visits_equal": bool(st_tile.visits == s64.visits),
+                      "status_equal": list(st_tile.status) == list(s64.status)}}
     del d_map, res
     torch.cuda.empty_cache()
     GG = 512
@@ -898,6 +916,26 @@ def run_ours(args, pre=None):
                 "rms_rel_err": float(np.sqrt(np.mean(rel ** 2))) if rel.size else 0.0,
                 "zero_pixels_differ": int(((map64 == 0) != (mixed_map == 0)).sum()),
                 "visits_equal": bool(st64.visits == st.visits)}
+        # the same FP64 map with one shared location walk per pixel tile
+        # instead of the reference's walk from hull triangle 0 for every ray
+        mesh.set_location(sd.LOCATE_TILE)
+        step(p64)
+        torch.cuda.synchronize()
+        for a, b in e64:
+            flush.zero_()
+            a.record(stream)
+            step(p64)
+            b.record(stream)
+        torch.cuda.synchronize()
+        mesh.set_location(sd.LOCATE_PER_RAY)
+        ms64t = float(np.median([a.elapsed_time(b) for a, b in e64]))
+        st64t = mesh.last_stats()
+        fp64["tile_location"] = {
+            "rays_per_s": spec.rays / (ms64t / 1e3), "ms_per_map": ms64t,
+            "speedup_mixed_over_it": ms64t / float(np.median(step_ms)),
+            "map_equal": bool(np.array_equal(d_map.cpu().numpy(), map64)),
+            "visits_equal": bool(st64t.visits == st64.visits),
+            "status_equal": list(st64t.status) == list(st64.status)}
     # device-timed sections run while host Qhull for the others continues;
     # everything host-timed (e2e, the CPU baseline, serving latency) runs
     # after the pool has finished, on idle host cores

@@ -186,6 +186,19 @@ dtfe_status_t dtfe_autotune(dtfe_mesh_t mesh, const dtfe_map_params_t *p, int *b
 /* Select a variant explicitly (-1: the built-in default). */
 dtfe_status_t dtfe_set_variant(dtfe_mesh_t mesh, int variant);
 
+/* Point location of FP64 maps (src/dtfe.c:518-552, restarted from hull
+ * triangle 0 for every sample at src/dtfe.c:624).  PER_RAY, the default, is
+ * the reference's walk for every ray.  TILE walks once per pixel tile, for the
+ * rectangle holding all of the tile's samples, while every edge test has one
+ * outcome for the whole rectangle; each ray resumes from where the rectangle
+ * first straddled a test, with the steps already taken counted against its
+ * budget.  Every ray then reaches exactly the tet and status of its own walk
+ * (the maps, crossings and statuses are bit-identical), at a fraction of the
+ * steps where the projected hull is large.  Mixed maps always locate by tile.
+ * TILE needs fewer than 2^27 hull triangles (DTFE_ERR_UNSUPPORTED otherwise). */
+typedef enum { DTFE_LOCATE_PER_RAY = 0, DTFE_LOCATE_TILE = 1 } dtfe_locate_t;
+dtfe_status_t dtfe_set_location(dtfe_mesh_t mesh, int mode);
+
 /* Defaults used by the drop-in entry points of dtfe.h. */
 void dtfe_set_default_precision(int precision);
 int dtfe_get_default_precision(void);

@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libsdtfe_b200.so")
 DTFE_FP64, DTFE_MIXED = 0, 1
 AXIS_Z, AXIS_X, AXIS_Y = 0, 1, 2
 MESH_FIELD, MESH_NO_FP64_REC, MESH_LAZY = 1, 2, 4
+LOCATE_PER_RAY, LOCATE_TILE = 0, 1
 RAY_OK, RAY_MISS, RAY_NO_EXIT, RAY_PERTURB_MAX, RAY_BUDGET, RAY_LOC_BUDGET = range(6)
 N_RAY_STATUS = 6
 
@@ -170,6 +171,7 @@ def lib() -> ctypes.CDLL:
     L.dtfe_kernel_launches.restype = ctypes.c_ulonglong
     L.dtfe_autotune.argtypes = [_vp, ctypes.POINTER(MapParams), ctypes.POINTER(_i), _vp]
     L.dtfe_set_variant.argtypes = [_vp, _i]
+    L.dtfe_set_location.argtypes = [_vp, _i]
     L.dtfe_tetra_from_cells.argtypes = [_f64, _i32, _i32, ctypes.c_size_t, _i32]
     # batches and the serving loop
     L.dtfe_batch_create.argtypes = [ctypes.POINTER(BatchJob), _i, ctypes.c_uint, ctypes.POINTER(_vp)]
@@ -341,6 +343,12 @@ class Mesh:
 
     def set_variant(self, variant: int):
         _check(lib().dtfe_set_variant(self.h, variant))
+
+    def set_location(self, mode: int):
+        """FP64 maps' point location: LOCATE_PER_RAY (the reference's walk from
+        hull triangle 0 for every ray) or LOCATE_TILE (one shared walk per
+        pixel tile, resumed per ray; bit-identical results)."""
+        _check(lib().dtfe_set_location(self.h, mode))
 
     def last_stats(self) -> MapStats:
         st = MapStats()

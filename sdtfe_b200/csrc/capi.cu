@@ -269,6 +269,15 @@ dtfe_status_t dtfe_set_variant(dtfe_mesh_t h, int variant) {
   return DTFE_OK;
 }
 
+dtfe_status_t dtfe_set_location(dtfe_mesh_t h, int mode) {
+  if (!h) return set_error(DTFE_ERR_INVALID, "NULL mesh");
+  if (mode != DTFE_LOCATE_PER_RAY && mode != DTFE_LOCATE_TILE)
+    return set_error(DTFE_ERR_INVALID, "location mode %d not 0 (per ray) or 1 (tile)", mode);
+  std::lock_guard<std::mutex> lk(h->mu);
+  h->m.fp64_location = mode;
+  return DTFE_OK;
+}
+
 dtfe_status_t dtfe_autotune(dtfe_mesh_t h, const dtfe_map_params_t* p, int* best,
                             dtfe_variant_t* timings) {
   if (!h || !p) return set_error(DTFE_ERR_INVALID, "NULL argument");

@@ -75,6 +75,7 @@ struct Mesh {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool timed = false;       // ev0/ev1 bracket the last walk launch
   int tune32 = -1;          // mixed-map kernel variant chosen by the autotuner (-1: default)
+  int fp64_location = DTFE_LOCATE_PER_RAY;  // FP64 maps' point location (dtfe_locate_t)
   size_t bytes = 0;
 };
 

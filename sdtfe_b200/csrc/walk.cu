@@ -27,6 +27,7 @@ struct MapArgs64 {
   double dxy, offx, offy, offz, lz, scale, soff;
   WalkConf64 walk;
   int loc_budget;
+  const int2* __restrict__ loc;  // per-tile shared locations, or nullptr: every ray walks from triangle 0
   unsigned long long* __restrict__ stats;
   double* __restrict__ ray_rho;
   int* __restrict__ ray_crossed;
@@ -81,7 +82,8 @@ __device__ __forceinline__ void map_tile64(const MapArgs64& a, int tile, double*
       const double yt = y + sdtfe_sample_u01(a.walk.seed, (uint64_t)p, (uint32_t)s, 1) * a.scale;
       const uint64_t rid = (uint64_t)p * (uint64_t)a.S + (uint64_t)s;
       int ft = -1;
-      if (a.n_tri > 0) ft = locate64(a.tri, 0, xt, yt, a.loc_budget, &status);
+      if (a.loc) ft = locate_from_tile(a.tri, __ldg(a.loc + tile), xt, yt, a.loc_budget, &status);
+      else if (a.n_tri > 0) ft = locate64(a.tri, 0, xt, yt, a.loc_budget, &status);
       if (ft >= 0) {
         SurfaceAcc64 acc{a.offz, a.offz + a.lz, 0.0};
         status = walk64(a.rec, ft, xt, yt, a.walk, rid, acc, &crossed, nullptr, 0);
@@ -115,6 +117,14 @@ __global__ void __launch_bounds__(256) k_map64(const MapArgs64 a) {
   extern __shared__ double s_val[];  // P*S doubles, then P*S bytes of success flags
   unsigned char* s_ok = reinterpret_cast<unsigned char*>(s_val + a.TW * a.TH * a.S);
   map_tile64(a, blockIdx.x, s_val, s_ok);
+}
+
+// Every tile's shared point location (tile_location), one thread per tile,
+// before a map whose mesh asked for tile-shared location.
+__global__ void __launch_bounds__(128) k_locate_map64(const MapArgs64 a, int n_tiles,
+                                                      int2* __restrict__ loc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n_tiles) loc[t] = tile_location(a, t);
 }
 
 // Persistent batch over several maps (see k_batch32 in walk32.cu): thread 0
@@ -289,6 +299,7 @@ static dtfe_status_t map_args64(Mesh& m, const MapGeom& g, double* d_map,
   a.soff = g.soff;
   a.walk = WalkConf64{g.lz, g.dist, g.seed, g.max_visits};
   a.loc_budget = 4 * A.n_tri + 64;
+  a.loc = nullptr;
   a.stats = stats;
   a.ray_rho = ray_rho;
   a.ray_crossed = ray_crossed;
@@ -308,11 +319,25 @@ dtfe_status_t launch_map64(Mesh& m, const MapGeom& g, double* d_map, cudaStream_
   if (smem > 48 * 1024)
     SDTFE_CUDA(cudaFuncSetAttribute(k_map64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long blocks = (long long)a.tiles_x * tiles_y;
+  const bool tile_loc = m.fp64_location == DTFE_LOCATE_TILE && a.n_tri > 0;
+  if (tile_loc && a.n_tri >= (1 << 27))
+    return set_error(DTFE_ERR_UNSUPPORTED,
+                     "tile-shared location over %d hull triangles (at most 2^27 - 1)", a.n_tri);
   SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
   SDTFE_CUDA(cudaEventRecord(m.ev0, s));
+  void* loc = nullptr;
+  if (tile_loc) {
+    SDTFE_TRY(scratch_alloc_async(&loc, kLocBytes * (size_t)blocks, s));
+    k_locate_map64<<<(unsigned)((blocks + 127) / 128), 128, 0, s>>>(a, (int)blocks,
+                                                                    static_cast<int2*>(loc));
+    count_launch();
+    a.loc = static_cast<const int2*>(loc);
+  }
   k_map64<<<(unsigned)blocks, threads, smem, s>>>(a);
   count_launch();
-  SDTFE_CUDA(cudaGetLastError());
+  const cudaError_t e = cudaGetLastError();
+  if (loc) scratch_free_async(loc, s);
+  SDTFE_CUDA(e);
   SDTFE_CUDA(cudaEventRecord(m.ev1, s));
   m.timed = true;
   return DTFE_OK;

@@ -949,34 +949,6 @@ __device__ __forceinline__ void add_stats32(unsigned long long* stats, bool acti
   }
 }
 
-// The rectangle holding every sample position of a tile.  A ray's position
-// is x(col) + u * scale with u in [0, 1), x(col) the expression below (the
-// same as the rays'); each is monotone in col and u, so the tile's positions
-// lie in [x(tx0), x(c1) + scale], and the same for y.
-__device__ __forceinline__ void tile_rect(const MapArgs32& a, int tile, double* xlo, double* xhi,
-                                          double* ylo, double* yhi) {
-  const int tx0 = (tile % a.tiles_x) * a.TW, ty0 = (tile / a.tiles_x) * a.TH;
-  const int c1 = min(tx0 + a.TW, a.G) - 1, r1 = min(ty0 + a.TH, a.G) - 1;
-  *xlo = tx0 * a.dxy + a.offx - a.soff;
-  *xhi = (c1 * a.dxy + a.offx - a.soff) + a.scale;
-  *ylo = ty0 * a.dxy + a.offy - a.soff;
-  *yhi = (r1 * a.dxy + a.offy - a.soff) + a.scale;
-}
-
-// A tile's shared point location (locate_region), packed for the map kernel:
-// (kind | steps << 2 as unsigned bits, start triangle).  steps <= loc_budget
-// = 4 n_tri + 64 < 2^29 + 64 (map_args32 caps n_tri below 2^27), so the
-// packed value fits in 32 unsigned bits; it is unpacked with unsigned shifts.
-__device__ __forceinline__ int2 tile_location(const MapArgs32& a, int tile) {
-  int kind = kLocMiss, start = -1, steps = 0;
-  if (a.n_tri > 0) {
-    double xlo, xhi, ylo, yhi;
-    tile_rect(a, tile, &xlo, &xhi, &ylo, &yhi);
-    kind = locate_region(a.tri, xlo, xhi, ylo, yhi, a.loc_budget, &start, &steps);
-  }
-  return make_int2((int)((unsigned)kind | ((unsigned)steps << 2)), start);
-}
-
 // One tile of one map: TW x TH pixels x S samples on BLOCK threads, one ray
 // per (pixel, sample), the S rays of a pixel in neighbouring lanes; the pixel
 // means are formed in sample order from shared memory (src/dtfe.c:615-645).
@@ -1004,17 +976,8 @@ __device__ __forceinline__ void map_tile32(const MapArgs32& a, int tile,
       const double xt = x + sdtfe_sample_u01(a.C.seed, (uint64_t)p, (uint32_t)s, 0) * a.scale;
       const double yt = y + sdtfe_sample_u01(a.C.seed, (uint64_t)p, (uint32_t)s, 1) * a.scale;
       const uint64_t rid = (uint64_t)p * (uint64_t)a.S + (uint64_t)s;
-      int ft = -1, ft_tri = -1;
-      const int2 l = __ldg(loc);
-      const int lk = (int)((unsigned)l.x & 3u);
-      if (lk == kLocFound) {
-        ft = __ldg(&a.tri[l.y].nb.w);
-        ft_tri = l.y;
-        status = kRayOk;
-      } else if (lk == kLocResume) {
-        ft = locate64(a.tri, l.y, xt, yt, a.loc_budget - (int)((unsigned)l.x >> 2), &status,
-                      &ft_tri);
-      }  // else every ray of the tile leaves the hull (or there is none): a miss
+      int ft_tri = -1;
+      int ft = locate_from_tile(a.tri, __ldg(loc), xt, yt, a.loc_budget, &status, &ft_tri);
       if (ft >= 0)
         status = walk32(a.rec, a.C, ft, ft_tri, xt, yt, rid, lut, &v, &crossed, &fb, nullptr, 0);
       if (status != kRayOk) v = 0.0;

@@ -282,6 +282,57 @@ __host__ __device__ inline int locate_region(const TriRec64* tri, double xlo, do
   return kLocResume;
 }
 
+// The rectangle holding every sample position of a map tile (Args: the FP64
+// or the mixed map's kernel arguments).  A ray's position is x(col) + u *
+// scale with u in [0, 1), x(col) the expression below (the same as the
+// rays'); each is monotone in col and u, so the tile's positions lie in
+// [x(tx0), x(c1) + scale], and the same for y.
+template <class Args>
+__device__ __forceinline__ void tile_rect(const Args& a, int tile, double* xlo, double* xhi,
+                                          double* ylo, double* yhi) {
+  const int tx0 = (tile % a.tiles_x) * a.TW, ty0 = (tile / a.tiles_x) * a.TH;
+  const int c1 = min(tx0 + a.TW, a.G) - 1, r1 = min(ty0 + a.TH, a.G) - 1;
+  *xlo = tx0 * a.dxy + a.offx - a.soff;
+  *xhi = (c1 * a.dxy + a.offx - a.soff) + a.scale;
+  *ylo = ty0 * a.dxy + a.offy - a.soff;
+  *yhi = (r1 * a.dxy + a.offy - a.soff) + a.scale;
+}
+
+// A tile's shared point location (locate_region), packed for the map kernel:
+// (kind | steps << 2 as unsigned bits, start triangle).  steps <= loc_budget
+// = 4 n_tri + 64 < 2^29 + 64 (the launchers cap n_tri below 2^27), so the
+// packed value fits in 32 unsigned bits; it is unpacked with unsigned shifts.
+template <class Args>
+__device__ __forceinline__ int2 tile_location(const Args& a, int tile) {
+  int kind = kLocMiss, start = -1, steps = 0;
+  if (a.n_tri > 0) {
+    double xlo, xhi, ylo, yhi;
+    tile_rect(a, tile, &xlo, &xhi, &ylo, &yhi);
+    kind = locate_region(a.tri, xlo, xhi, ylo, yhi, a.loc_budget, &start, &steps);
+  }
+  return make_int2((int)((unsigned)kind | ((unsigned)steps << 2)), start);
+}
+
+// One ray's point location from its tile's shared walk l (tile_location):
+// where the tile's rectangle straddled a test, the ray resumes the walk from
+// triangle 0 at that triangle with the steps already taken counted against
+// its budget, so it reaches exactly the tet, triangle and status of its own
+// locate64(tri, 0, ...).  A tile that left the hull leaves every ray a miss.
+__device__ __forceinline__ int locate_from_tile(const TriRec64* __restrict__ tri, int2 l,
+                                                double qx, double qy, int loc_budget,
+                                                int* status, int* tri_out = nullptr) {
+  const int lk = (int)((unsigned)l.x & 3u);
+  if (lk == kLocFound) {
+    if (tri_out) *tri_out = l.y;
+    *status = kRayOk;
+    return __ldg(&tri[l.y].nb.w);
+  }
+  if (lk == kLocResume)
+    return locate64(tri, l.y, qx, qy, loc_budget - (int)((unsigned)l.x >> 2), status, tri_out);
+  *status = kRayMiss;
+  return -1;
+}
+
 // ---------------------------------------------------------------------------
 // Accumulators: what a walk does with each crossed tet.
 

@@ -86,6 +86,21 @@ def test_config1_fp64_map_and_rays_bit_exact(config1, sd, oracle):
     assert abs(mass / len(pos4) - 1.0) < 2e-3
 
 
+def test_config1_fp64_tile_location_bit_exact(config1, sd):
+    """Config 1 with tile-shared location: the same map and rays as the
+    reference's per-ray location walk."""
+    pos4, tetra, spec, prep, m = config1
+    want = m.map(_params(sd, spec, sd.DTFE_FP64), per_ray=True)
+    m.set_location(sd.LOCATE_TILE)
+    try:
+        got = m.map(_params(sd, spec, sd.DTFE_FP64), per_ray=True)
+    finally:
+        m.set_location(sd.LOCATE_PER_RAY)
+    for k in (0, 2, 3, 4):
+        assert np.array_equal(got[k], want[k])
+    assert got[1].visits == want[1].visits
+
+
 def test_config1_mixed_same_crossings_within_tolerance(config1, sd):
     pos4, tetra, spec, prep, m = config1
     g64, s64, r64, c64, t64 = m.map(_params(sd, spec, sd.DTFE_FP64), per_ray=True)
@@ -150,6 +165,22 @@ def test_clustered_full_box_fp64_bit_exact_and_mass(clustered, sd, oracle):
     px = (1.0 / G) ** 2
     assert abs(got.sum() * px / len(pos4) - 1.0) < 1e-2
     assert abs(mix.sum() / got.sum() - 1.0) < 1e-7
+
+
+def test_clustered_fp64_tile_location_bit_exact(clustered, sd):
+    """The clustered recipe at 512 x 512 x 16 (tiles along the hull's edges
+    included): tile-shared location gives the per-ray walk's rays exactly."""
+    pos4, tetra, prep, m = clustered
+    p = sd.map_params(512, 1.0, 1.0, (0.5, 0.5, 0.5), 16, 0.0, SEED)
+    want = m.map(p, per_ray=True)
+    m.set_location(sd.LOCATE_TILE)
+    try:
+        got = m.map(p, per_ray=True)
+    finally:
+        m.set_location(sd.LOCATE_PER_RAY)
+    for k in (0, 2, 3, 4):
+        assert np.array_equal(got[k], want[k])
+    assert list(got[1].status) == list(want[1].status)
 
 
 def test_clustered_window_at_single_map_pixel_size(clustered, sd):

@@ -62,6 +62,20 @@ def test_map_accumulates(gmesh, sd):
     assert np.array_equal(got, base + s["map"])
 
 
+def test_map_fp64_tile_location(gmesh, sd):
+    """One shared location walk per pixel tile (dtfe_set_location) leaves the
+    FP64 maps equal to the reference's, lattice degeneracies included."""
+    s, m = gmesh
+    m.set_location(sd.LOCATE_TILE)
+    try:
+        got, _ = m.map(sd.map_params(24, 1.0, 1.0, (0.5, 0.5, 0.5), 4, 0.0, SEED))
+        assert np.array_equal(got, s["map"])
+        got2, _ = m.map(sd.map_params(20, 0.6, 0.5, (0.45, 0.55, 0.5), 3, 0.05, SEED + 1))
+        assert np.array_equal(got2, s["map2"])
+    finally:
+        m.set_location(sd.LOCATE_PER_RAY)
+
+
 def test_trace_visits(gmesh, sd):
     s, m = gmesh
     p = sd.map_params(24, 1.0, 1.0, (0.5, 0.5, 0.5), 4, 0.0, SEED)
@@ -110,6 +124,34 @@ def test_medium_map_vs_oracle(medium, sd, oracle, G, S, box, boxz, ds):
     assert np.array_equal(got, want)
     assert st.visits == int(rc.sum())
     assert list(st.status) == [int((rs == k).sum()) for k in range(6)]
+
+
+@pytest.mark.parametrize("G,S,box,c", [(64, 4, 1.0, (0.5, 0.48, 0.52)), (45, 3, 1.5, (0.5, 0.5, 0.5)),
+                                       (33, 5, 0.4, (0.95, 0.05, 0.5)), (16, 33, 0.5, (0.3, 0.6, 0.5))])
+def test_medium_tile_location_vs_oracle(medium, sd, oracle, G, S, box, c):
+    """FP64 maps with tile-shared location against the oracle's walk from
+    triangle 0 for every ray: maps, ray integrals, crossings and statuses
+    equal, on windows inside the hull, around it and across its corner."""
+    pos4, tetra, prep, m = medium
+    want, rr, rc, rs = oracle.map(prep, G, box, 1.0, c, S, 0.0, 7, per_ray=True)
+    m.set_location(sd.LOCATE_TILE)
+    try:
+        got, st, gr, gc, gs = m.map(sd.map_params(G, box, 1.0, c, S, 0.0, 7), per_ray=True)
+    finally:
+        m.set_location(sd.LOCATE_PER_RAY)
+    assert np.array_equal(got, want)
+    assert np.array_equal(gr, rr)
+    assert np.array_equal(gc, rc)
+    assert np.array_equal(gs, rs)
+    if box > 1.0 or c[0] > 0.9:
+        assert (rs == sd.RAY_MISS).any() and (rs == sd.RAY_OK).any()
+
+
+def test_location_mode_rejected(medium, sd):
+    pos4, tetra, prep, m = medium
+    for bad in (-1, 2):
+        with pytest.raises(sd.DTFEError):
+            m.set_location(bad)
 
 
 @pytest.mark.parametrize("axis", [1, 2])
