@@ -221,11 +221,12 @@ void dtfe_set_seed(uint64_t seed);
  * loading that is also when the 48 MiB are reserved on the device, which
  * then holds them until the process exits.  So make one call per device at
  * start-up - a call with n_particles == 0 does the set-up alone - before a
- * memory pool takes the device's memory and before any stream capture.  All
+ * memory pool takes the device's memory.  All
  * calls share the array, so calls that overlap on the GPU (other streams,
  * other host threads) race.  The call blocks: it reads a validation flag
  * back mid-call and returns after its work on `stream` (NULL: the default
- * stream), which it orders after the stream's earlier work, has finished. */
+ * stream), which it orders after the stream's earlier work, has finished;
+ * so no call can be captured into a CUDA graph. */
 dtfe_status_t dtfe_density_noalloc(const double *d_particle_data, int n_particles,
                                    const int *d_tetra_data, int n_tetra, float p_mass,
                                    double *d_rho, void *stream);
