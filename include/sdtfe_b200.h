@@ -123,6 +123,10 @@ const char *dtfe_status_string(dtfe_status_t s);
 dtfe_status_t dtfe_mesh_create(const double *particle_data, int n_particles,
                                const int *tetra_data, int n_tetra, float p_mass,
                                unsigned flags, dtfe_mesh_t *out);
+/* Releases the mesh's device memory, stream-ordered on the handle's own
+ * stream (no device-wide synchronisation), into a pool that keeps it for the
+ * next mesh.  Work the caller enqueued on its own streams with the mesh
+ * (dtfe_map_device, dtfe_grid_device, batches) must have finished first. */
 dtfe_status_t dtfe_mesh_destroy(dtfe_mesh_t mesh);
 dtfe_status_t dtfe_mesh_info(dtfe_mesh_t mesh, dtfe_mesh_info_t *info);
 dtfe_status_t dtfe_mesh_sync(dtfe_mesh_t mesh);

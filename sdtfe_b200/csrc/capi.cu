@@ -333,25 +333,61 @@ dtfe_status_t dtfe_mesh_last_stats(dtfe_mesh_t h, dtfe_map_stats_t* st) {
   return read_stats(h->m, st);
 }
 
-dtfe_status_t dtfe_map(dtfe_mesh_t h, const dtfe_map_params_t* p, double* map,
-                       dtfe_map_stats_t* stats) {
-  if (!h || !map) return set_error(DTFE_ERR_INVALID, "NULL argument");
-  std::lock_guard<std::mutex> lk(h->mu);
-  Mesh& m = h->m;
+extern "C++" {
+namespace {
+
+// A map into a host array, accumulated into as the reference does: the array
+// is uploaded, the walk enqueued, while_walking() run on the host while the
+// walk runs, and the array downloaded.  With the handle's lock held.
+template <class F>
+dtfe_status_t map_to_host(Mesh& m, const dtfe_map_params_t* p, double* map, F&& while_walking) {
   SDTFE_TRY(check_params(m, p));
   SDTFE_TRY(prepare_axis(m, p->axis, p->precision));
   cudaStream_t s = m.stream;
   const size_t bytes = sizeof(double) * (size_t)p->grid_dim * p->grid_dim;
   double* d_map = nullptr;
   SDTFE_CUDA(cudaMallocAsync(&d_map, bytes, s));
-  SDTFE_CUDA(cudaMemcpyAsync(d_map, map, bytes, cudaMemcpyHostToDevice, s));
-  dtfe_status_t st = launch_map(m, p, d_map, s);
+  cudaError_t e = cudaMemcpyAsync(d_map, map, bytes, cudaMemcpyHostToDevice, s);
+  dtfe_status_t st = e == cudaSuccess ? launch_map(m, p, d_map, s)
+                                      : set_error(DTFE_ERR_CUDA, "map: %s", cudaGetErrorString(e));
+  if (st == DTFE_OK) st = while_walking();
   if (st == DTFE_OK) {
-    cudaError_t e = cudaMemcpyAsync(map, d_map, bytes, cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(map, d_map, bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = set_error(DTFE_ERR_CUDA, "map: %s", cudaGetErrorString(e));
   }
   cudaFreeAsync(d_map, s);
+  return st;
+}
+
+dtfe_status_t nothing_else() { return DTFE_OK; }
+
+// Column 3 of the caller's particle array receives the densities, as
+// pre_compute_vol does (src/triangulate.c:183-225).  The device's rows
+// (x, y, z, rho) are the caller's rows with column 3 replaced, so they are
+// copied back whole, on a stream of their own, while the walk enqueued before
+// runs.  Returns when the copy is done.
+dtfe_status_t copy_back_densities(Mesh& m, double* particle_data) {
+  if (m.n == 0) return DTFE_OK;
+  cudaStream_t side = nullptr;
+  SDTFE_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  cudaError_t e = cudaMemcpyAsync(particle_data, m.pos, sizeof(double4) * (size_t)m.n,
+                                  cudaMemcpyDeviceToHost, side);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(side);
+  cudaStreamDestroy(side);
+  SDTFE_CUDA(e);
+  return DTFE_OK;
+}
+
+}  // namespace
+}  // extern "C++"
+
+dtfe_status_t dtfe_map(dtfe_mesh_t h, const dtfe_map_params_t* p, double* map,
+                       dtfe_map_stats_t* stats) {
+  if (!h || !map) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  Mesh& m = h->m;
+  dtfe_status_t st = map_to_host(m, p, map, nothing_else);
   if (st == DTFE_OK && stats) st = read_stats(m, stats);
   return st;
 }
@@ -482,12 +518,12 @@ dtfe_status_t launch_grid(Mesh& m, int G, double box_len, const double center[3]
 
 }  // namespace
 
-dtfe_status_t dtfe_grid_ex(dtfe_mesh_t h, int G, double box_len, const double center[3],
-                           unsigned ss, uint64_t seed, int precision, double* grid) {
-  SDTFE_TRY(check_grid(h, G, box_len, center, ss, precision));
-  if (!grid) return set_error(DTFE_ERR_INVALID, "NULL argument");
-  std::lock_guard<std::mutex> lk(h->mu);
-  Mesh& m = h->m;
+extern "C++" {
+// The grid into a host array, accumulated into (src/dtfe.c:505-511), with
+// while_walking() run on the host while the walk runs; as map_to_host.
+template <class F>
+dtfe_status_t grid_to_host(Mesh& m, int G, double box_len, const double center[3], unsigned ss,
+                           uint64_t seed, int precision, double* grid, F&& while_walking) {
   cudaStream_t s = m.stream;
   const size_t bytes = sizeof(double) * (size_t)G * G * G;
   double* d = nullptr;
@@ -495,6 +531,7 @@ dtfe_status_t dtfe_grid_ex(dtfe_mesh_t h, int G, double box_len, const double ce
   cudaError_t e = cudaMemcpyAsync(d, grid, bytes, cudaMemcpyHostToDevice, s);
   dtfe_status_t st = e == cudaSuccess ? launch_grid(m, G, box_len, center, ss, seed, precision, d, s)
                                       : set_error(DTFE_ERR_CUDA, "grid: %s", cudaGetErrorString(e));
+  if (st == DTFE_OK) st = while_walking();
   if (st == DTFE_OK) {
     e = cudaMemcpyAsync(grid, d, bytes, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -502,6 +539,15 @@ dtfe_status_t dtfe_grid_ex(dtfe_mesh_t h, int G, double box_len, const double ce
   }
   cudaFreeAsync(d, s);
   return st;
+}
+}  // extern "C++"
+
+dtfe_status_t dtfe_grid_ex(dtfe_mesh_t h, int G, double box_len, const double center[3],
+                           unsigned ss, uint64_t seed, int precision, double* grid) {
+  SDTFE_TRY(check_grid(h, G, box_len, center, ss, precision));
+  if (!grid) return set_error(DTFE_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(h->mu);
+  return grid_to_host(h->m, G, box_len, center, ss, seed, precision, grid, nothing_else);
 }
 
 dtfe_status_t dtfe_grid(dtfe_mesh_t h, int G, double box_len, const double center[3],
@@ -543,12 +589,11 @@ void compute_density(double* particle_data, int n_particles, int* tetra_data, in
   p.seed = call_seed();
   p.axis = DTFE_AXIS_Z;
   p.precision = dtfe_get_default_precision();
-  // column 3 of the caller's array receives the densities, as pre_compute_vol does
-  std::vector<double> dens(n_particles > 0 ? n_particles : 0);
-  dtfe_status_t s = n_particles ? dtfe_mesh_density(h, dens.data()) : DTFE_OK;
-  if (s == DTFE_OK)
-    for (int i = 0; i < n_particles; ++i) particle_data[4 * (size_t)i + 3] = dens[i];
-  if (s == DTFE_OK) s = dtfe_map(h, &p, rho, nullptr);
+  dtfe_status_t s;
+  {
+    std::lock_guard<std::mutex> lk(h->mu);
+    s = map_to_host(h->m, &p, rho, [&] { return copy_back_densities(h->m, particle_data); });
+  }
   if (s != DTFE_OK) report("compute_density");
   dtfe_mesh_destroy(h);
 }
@@ -573,14 +618,14 @@ void compute_3d_density(double* particle_data, int n_particles, int* tetra_data,
   dtfe_mesh_t h = nullptr;
   if (dtfe_mesh_create(particle_data, n_particles, tetra_data, n_tetra, p_mass, 0, &h) != DTFE_OK)
     return report("compute_3d_density");
-  std::vector<double> dens(n_particles > 0 ? n_particles : 0);
-  dtfe_status_t s = n_particles ? dtfe_mesh_density(h, dens.data()) : DTFE_OK;
-  if (s == DTFE_OK)
-    for (int i = 0; i < n_particles; ++i) particle_data[4 * (size_t)i + 3] = dens[i];
   const double c[3] = {center_x, center_y, center_z};
-  if (s == DTFE_OK)
-    s = dtfe_grid_ex(h, grid_dim, box_len, c, supersampling, call_seed(),
-                     dtfe_get_default_precision(), rho);
+  const int precision = dtfe_get_default_precision();
+  dtfe_status_t s = check_grid(h, grid_dim, box_len, c, supersampling, precision);
+  if (s == DTFE_OK) {
+    std::lock_guard<std::mutex> lk(h->mu);
+    s = grid_to_host(h->m, grid_dim, box_len, c, supersampling, call_seed(), precision, rho,
+                     [&] { return copy_back_densities(h->m, particle_data); });
+  }
   if (s != DTFE_OK) report("compute_3d_density");
   dtfe_mesh_destroy(h);
 }

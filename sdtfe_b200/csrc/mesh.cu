@@ -389,19 +389,12 @@ dtfe_status_t exclusive_scan(const int* in, int* out, int n, cudaStream_t s) {
   return DTFE_OK;
 }
 
-template <class T>
-dtfe_status_t dmalloc(T** p, size_t count, Mesh* m) {
-  *p = nullptr;
-  if (count == 0) count = 1;
-  SDTFE_CUDA(cudaMalloc((void**)p, count * sizeof(T)));
-  m->bytes += count * sizeof(T);
-  return DTFE_OK;
-}
-
-// The walk records' memory pool of each device: stream-ordered allocation (no
-// device-wide synchronisation when records are built or dropped while maps
-// run), and freed record memory kept for reuse up to an eighth of the device
-// (at most 16 GB) instead of being unmapped and mapped again by every mesh.
+// The meshes' memory pool of each device (vertices, rows, gradients,
+// adjacency, walk records, per-call scratch): stream-ordered allocation (no
+// device-wide synchronisation when a mesh is built or destroyed, or records
+// are built or dropped, while maps run), and freed memory kept for reuse up
+// to an eighth of the device (at most 16 GB) instead of being unmapped and
+// mapped again by every mesh.
 constexpr int kMaxPoolDevices = 64;
 std::mutex g_pool_mu;
 cudaMemPool_t g_record_pool[kMaxPoolDevices] = {};
@@ -474,15 +467,6 @@ void dfree_async(T*& p, size_t count, Mesh* m) {
   p = nullptr;
 }
 
-template <class T>
-void dfree(T*& p, size_t count, Mesh* m) {
-  if (p) {
-    cudaFree(p);
-    m->bytes -= (count ? count : 1) * sizeof(T);
-  }
-  p = nullptr;
-}
-
 }  // namespace
 
 dtfe_status_t mesh_upload(Mesh* m, const double* particle_data, int n, const int* tetra_data,
@@ -496,9 +480,9 @@ dtfe_status_t mesh_upload(Mesh* m, const double* particle_data, int n, const int
   SDTFE_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
   SDTFE_CUDA(cudaEventCreate(&m->ev0));
   SDTFE_CUDA(cudaEventCreate(&m->ev1));
-  SDTFE_TRY(dmalloc(&m->pos, n, m));
-  SDTFE_TRY(dmalloc(&m->rows, 2 * (size_t)nt, m));
-  SDTFE_TRY(dmalloc(&m->stats, kStatCount, m));
+  SDTFE_TRY(dmalloc_async(&m->pos, n, m));
+  SDTFE_TRY(dmalloc_async(&m->rows, 2 * (size_t)nt, m));
+  SDTFE_TRY(dmalloc_async(&m->stats, kStatCount, m));
   cudaStream_t s = m->stream;
   if (n) SDTFE_CUDA(cudaMemcpyAsync(m->pos, particle_data, sizeof(double4) * n, cudaMemcpyHostToDevice, s));
   if (nt) SDTFE_CUDA(cudaMemcpyAsync(m->rows, tetra_data, sizeof(int4) * 2 * (size_t)nt, cudaMemcpyHostToDevice, s));
@@ -534,7 +518,7 @@ dtfe_status_t mesh_upload(Mesh* m, const double* particle_data, int n, const int
 dtfe_status_t mesh_density(Mesh* m) {
   cudaStream_t s = m->stream;
   const int n = m->n, nt = m->nt;
-  SDTFE_TRY(dmalloc(&m->adj, n, m));
+  SDTFE_TRY(dmalloc_async(&m->adj, n, m));
   double* vol = nullptr;
   int *cnt = nullptr, *off = nullptr, *idx = nullptr;
   SDTFE_CUDA(cudaMallocAsync(&vol, sizeof(double) * (nt ? nt : 1), s));
@@ -572,7 +556,7 @@ dtfe_status_t mesh_density(Mesh* m) {
 }
 
 dtfe_status_t mesh_gradients(Mesh* m) {
-  if (!m->grad) SDTFE_TRY(dmalloc(&m->grad, 3 * (size_t)m->nt, m));
+  if (!m->grad) SDTFE_TRY(dmalloc_async(&m->grad, 3 * (size_t)m->nt, m));
   if (m->nt) {
     k_gradients<<<grid_for(m->nt), kBlock, 0, m->stream>>>(m->pos, m->rows, m->nt, m->grad);
     count_launch();
@@ -709,25 +693,13 @@ dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count
   int n_tri = 0;
   SDTFE_CUDA(cudaMemcpyAsync(&n_tri, off + nt, sizeof(int), cudaMemcpyDeviceToHost, s));
   SDTFE_CUDA(cudaStreamSynchronize(s));
-  // replace the axis' triangles
-  if (A.tri) {
-    cudaFree(A.tri);
-    m->bytes -= sizeof(TriRec64) * (size_t)(A.n_tri ? A.n_tri : 1);
-    A.tri = nullptr;
-  }
-  if (A.tri_rows) {
-    cudaFree(A.tri_rows);
-    m->bytes -= sizeof(int) * 8 * (size_t)(A.n_tri ? A.n_tri : 1);
-    A.tri_rows = nullptr;
-  }
-  if (A.tri_face) {
-    cudaFree(A.tri_face);
-    m->bytes -= (size_t)(A.n_tri ? A.n_tri : 1);
-    A.tri_face = nullptr;
-  }
-  SDTFE_TRY(dmalloc(&A.tri, n_tri, m));
-  SDTFE_TRY(dmalloc(&A.tri_rows, 8 * (size_t)n_tri, m));
-  SDTFE_TRY(dmalloc(&A.tri_face, n_tri, m));
+  // replace the axis' triangles (the mesh stream is idle: synchronised above)
+  dfree_async(A.tri, A.n_tri, m);
+  dfree_async(A.tri_rows, 8 * (size_t)A.n_tri, m);
+  dfree_async(A.tri_face, A.n_tri, m);
+  SDTFE_TRY(dmalloc_async(&A.tri, n_tri, m));
+  SDTFE_TRY(dmalloc_async(&A.tri_rows, 8 * (size_t)n_tri, m));
+  SDTFE_TRY(dmalloc_async(&A.tri_face, n_tri, m));
   A.n_tri = n_tri;
   if (nt) {
     k_hull_emit<<<grid_for(nt), kBlock, 0, s>>>(m->rows, nt, mask, off, A.tri_rows, A.tri_face);
@@ -764,23 +736,24 @@ dtfe_status_t mesh_hull(Mesh* m, int axis, const uint32_t* host_mask, int* count
 }
 
 void mesh_free(Mesh* m) {
-  // stream-ordered frees first, so that the synchronisation covers them
+  // every array returns to the pool stream-ordered on the mesh stream, which
+  // is then synchronised (the caller's own streams are done with the mesh)
   for (auto& A : m->ax) {
     dfree_async(A.rec64, m->nt, m);
     dfree_async(A.rot32, 4 * (size_t)m->nt, m);
   }
   dfree_async(m->fld64, m->nt, m);
-  if (m->stream) cudaStreamSynchronize(m->stream);
-  dfree(m->pos, m->n, m);
-  dfree(m->rows, 2 * (size_t)m->nt, m);
-  dfree(m->grad, 3 * (size_t)m->nt, m);
-  dfree(m->adj, m->n, m);
-  dfree(m->stats, kStatCount, m);
+  dfree_async(m->pos, m->n, m);
+  dfree_async(m->rows, 2 * (size_t)m->nt, m);
+  dfree_async(m->grad, 3 * (size_t)m->nt, m);
+  dfree_async(m->adj, m->n, m);
+  dfree_async(m->stats, kStatCount, m);
   for (auto& A : m->ax) {
-    dfree(A.tri, A.n_tri, m);
-    dfree(A.tri_rows, 8 * (size_t)A.n_tri, m);
-    dfree(A.tri_face, A.n_tri, m);
+    dfree_async(A.tri, A.n_tri, m);
+    dfree_async(A.tri_rows, 8 * (size_t)A.n_tri, m);
+    dfree_async(A.tri_face, A.n_tri, m);
   }
+  if (m->stream) cudaStreamSynchronize(m->stream);
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
   if (m->stream) cudaStreamDestroy(m->stream);

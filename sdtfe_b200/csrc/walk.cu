@@ -206,11 +206,11 @@ __global__ void __launch_bounds__(128) k_grid64(const TetRec64* __restrict__ rec
                                                 double box_len, int ss, WalkConf64 walk,
                                                 int loc_budget, double* __restrict__ grid,
                                                 unsigned long long* __restrict__ stats) {
-  const long long cidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = cidx < (long long)G * G;
+  int i, j;
+  const bool active = grid_column(G, &i, &j);
+  const long long cidx = (long long)i * G + j;
   int worst = kRayOk, visits = 0;
   if (active) {
-    const int i = (int)(cidx / G), j = (int)(cidx % G);
     const double ds = dxy / ss;
     ColumnAcc64 acc;
     acc.col = grid + (size_t)cidx * G;
@@ -431,12 +431,10 @@ dtfe_status_t launch_grid64(Mesh& m, int G, double box_len, const double center[
   const double offy = -(box_len / 2.0) + center[1];
   const double offz = -(box_len / 2.0) + center[2];
   WalkConf64 w{box_len, (dxy / 2.0) / kPerturbMax, seed, max_visits};
-  const long long ncol = (long long)G * G;
   SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
   SDTFE_CUDA(cudaEventRecord(m.ev0, s));
-  k_grid64<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(A.rec64, A.tri, A.n_tri, G, dxy, offx,
-                                                          offy, offz, box_len, (int)ss, w,
-                                                          4 * A.n_tri + 64, d_grid, m.stats);
+  k_grid64<<<grid_blocks(G), 128, 0, s>>>(A.rec64, A.tri, A.n_tri, G, dxy, offx, offy, offz,
+                                          box_len, (int)ss, w, 4 * A.n_tri + 64, d_grid, m.stats);
   count_launch();
   SDTFE_CUDA(cudaGetLastError());
   SDTFE_CUDA(cudaEventRecord(m.ev1, s));

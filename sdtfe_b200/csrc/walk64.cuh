@@ -354,6 +354,28 @@ struct SurfaceAcc64 {
   }
 };
 
+// One node's value added into its grid cell, *cell += v, as a reduction
+// performed at L2: the thread does not wait for the cell's old value.  Each
+// grid column belongs to one thread, and one thread's reductions to one
+// address are performed in its program order, so every cell receives exactly
+// the additions, in the order and with the roundings, of the reference's
+// loop (src/dtfe.c:505-511).
+__device__ __forceinline__ void cell_add(double* cell, double v) { atomicAdd(cell, v); }
+
+// This thread's grid column (i: x index, j: y index) in a launch of
+// grid_blocks(G) blocks of 128 threads: a block covers 8 x 16 columns and
+// each of its warps a 4 x 8 patch, so that a warp's columns are neighbours
+// and cross many of the same tets.  False for the columns past the grid.
+__device__ __forceinline__ bool grid_column(int G, int* i, int* j) {
+  const int tiles_j = (G + 15) >> 4;
+  const int ti = (int)blockIdx.x / tiles_j, tj = (int)blockIdx.x - ti * tiles_j;
+  const int lane = (int)threadIdx.x & 31, wq = (int)threadIdx.x >> 5;
+  *i = ti * 8 + (wq >> 1) * 4 + (lane >> 3);
+  *j = tj * 16 + (wq & 1) * 8 + (lane & 7);
+  return *i < G && *j < G;
+}
+inline unsigned grid_blocks(int G) { return (unsigned)(((G + 7) / 8) * ((G + 15) / 16)); }
+
 // a12: 3-D column, src/dtfe.c:489-513.  The field is sampled at the fine z
 // nodes inside the chord and added, with weight 1/ss^3, to the column cell.
 struct ColumnAcc64 {
@@ -372,7 +394,7 @@ struct ColumnAcc64 {
       for (int is = i0; is < i1; ++is) {
         const int iz = (int)((unsigned)is / (unsigned)ss);
         const double zi = z0 + dzs * is + dzs / 2.;
-        col[iz] += (fixed + gz * zi) * w;
+        cell_add(col + iz, (fixed + gz * zi) * w);
       }
     }
   }

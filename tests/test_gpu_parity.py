@@ -180,6 +180,24 @@ def test_medium_grid_vs_oracle(medium, oracle):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("G,box,center", [(40, 1.0, (0.5, 0.5, 0.5)), (27, 1.3, (0.45, 0.5, 0.55))])
+def test_medium_grid_one_node_per_cell_vs_oracle(medium, sd, oracle, G, box, center):
+    """Supersampling 1 (one node per cell), onto a grid that already holds
+    values: each cell receives its node with the reference's one rounding,
+    cells outside the mesh keep theirs; both precisions cross the same tets."""
+    pos4, tetra, prep, m = medium
+    want, _ = oracle.grid(prep, G, box, center, 1, 9)
+    got = m.grid(G, box, center, 1, 9)
+    assert np.array_equal(got, want)
+    base = np.random.default_rng(3).random((G, G, G)) + 1.0
+    got = m.grid(G, box, center, 1, 9, out=base.copy())
+    assert np.array_equal(got, base + want)
+    st64 = m.last_stats()
+    g32 = m.grid(G, box, center, 1, 9, out=base.copy(), precision=sd.DTFE_MIXED)
+    assert m.last_stats().visits == st64.visits
+    assert np.max(np.abs(g32 - got) / np.abs(got)) <= 1e-5
+
+
 # --------------------------------------------------------------------------
 # drop-in entry points of dtfe.h / triangulate.h
 # --------------------------------------------------------------------------

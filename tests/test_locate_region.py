@@ -41,7 +41,8 @@ def lr():
     hdr = os.path.join(ROOT, "sdtfe_b200", "csrc", "walk64.cuh")
     if not os.path.exists(out) or os.path.getmtime(out) < max(os.path.getmtime(src),
                                                                os.path.getmtime(hdr)):
-        subprocess.run([nvcc, "-O2", "-std=c++17", "-shared", "-Wno-deprecated-gpu-targets",
+        subprocess.run([nvcc, "-O2", "-std=c++17", "-shared",
+                        "-gencode", "arch=compute_100a,code=sm_100a",
                         "-Xcompiler", "-fPIC,-ffp-contract=off",
                         "-I" + os.path.join(ROOT, "include"),
                         "-I" + os.path.join(ROOT, "sdtfe_b200", "csrc"), src, "-o", out],
