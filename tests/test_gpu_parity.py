@@ -213,6 +213,13 @@ def test_dropin_compute_density(golden, sd, oracle):
                           0.5, 0.5, 4, 0.0)
         assert np.array_equal(rho.reshape(24, 24), s["map"])
         assert np.array_equal(pd[:, 3], s["density"])  # column 3 overwritten in place
+        assert np.array_equal(pd[:, :3], s["pos4"][:, :3])  # the positions untouched
+        # the map is accumulated into, as the reference's rho[p] += ...
+        pd[:, 3] = 0.0
+        rho = np.full(24 * 24, 0.5)
+        L.compute_density(pd, len(pd), s["tetra"], len(s["tetra"]), 24, 1.0, 1.0, rho, 1.0, 0.5,
+                          0.5, 0.5, 4, 0.0)
+        assert np.array_equal(rho.reshape(24, 24), 0.5 + s["map"])
     finally:
         L.dtfe_set_seed(0)
 
