@@ -1012,12 +1012,9 @@ def run_ours(args, pre=None):
 
     run_section("plain_small",
                 lambda: section_plain_small(args, sd, torch, dev, stream, flush, tri))
-    # the large field before the serving loop's hundreds of GB of record
-    # builds and evictions: after them the latency-bound 3-D grid walk runs
-    # measurably slower on the device memory they leave
+    run_section("serving", lambda: section_serving(args, sd, torch, tri))
     run_section("large_field",
                 lambda: section_large_field(args, sd, torch, dev, stream, flush, tri))
-    run_section("serving", lambda: section_serving(args, sd, torch, tri))
     if tri is not None:
         extra["qhull_pool"] = tri.info()
 

@@ -650,7 +650,7 @@ struct ColumnAcc32 {
       for (int is = i0; is < i1; ++is) {
         const int iz = (int)((unsigned)is / (unsigned)ss);
         const double zi = z0 + dzs * is + dzs / 2.;
-        col[iz] += (base + yz.y * zi) * w;
+        cell_add(col + iz, (base + yz.y * zi) * w);
       }
     }
     i_in = i1u;
@@ -679,7 +679,7 @@ struct ColumnAcc32 {
     for (int is = i0; is < i1; ++is) {
       const int iz = (int)((unsigned)is / (unsigned)ss);
       const double zi = z0 + dzs * is + dzs / 2.;
-      col[iz] += (fixed + gz * zi) * w;
+      cell_add(col + iz, (fixed + gz * zi) * w);
     }
     ++*fallbacks;
   }
@@ -1143,11 +1143,11 @@ __global__ void __launch_bounds__(128) k_grid32(const __grid_constant__ GridArgs
   __shared__ unsigned char s_lut[kLutBytes];
   fill_lut(s_lut);
   __syncthreads();
-  const long long cidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = cidx < (long long)a.G * a.G;
+  int i, j;
+  const bool active = grid_column(a.G, &i, &j);
+  const long long cidx = (long long)i * a.G + j;
   int worst = kRayOk, visits = 0, fallbacks = 0;
   if (active) {
-    const int i = (int)(cidx / a.G), j = (int)(cidx % a.G);
     const double ds = a.dxy / a.ss;
     ColumnAcc32 acc;
     acc.col = a.grid + (size_t)cidx * a.G;
@@ -1367,10 +1367,9 @@ dtfe_status_t launch_grid32(Mesh& m, int G, double box_len, const double center[
   a.fld = m.fld64;
   a.grid = d_grid;
   a.stats = m.stats;
-  const long long ncol = (long long)G * G;
   SDTFE_CUDA(cudaMemsetAsync(m.stats, 0, sizeof(unsigned long long) * kStatCount, s));
   SDTFE_CUDA(cudaEventRecord(m.ev0, s));
-  k_grid32<<<(unsigned)((ncol + 127) / 128), 128, 0, s>>>(a);
+  k_grid32<<<grid_blocks(G), 128, 0, s>>>(a);
   count_launch();
   SDTFE_CUDA(cudaGetLastError());
   SDTFE_CUDA(cudaEventRecord(m.ev1, s));
