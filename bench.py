@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--sections", default="plain_small,batch,serving,large_field",
                     help="extra sections on one GPU: batch (64 cutouts in one persistent launch), "
                          "serving (request stream with continuous batching); 'none' to skip")
+    ap.add_argument("--large-side", type=int, default=192,
+                    help="lattice side of the large field (192: the 9.2M-point configuration; "
+                         "smaller sides make profiling cases of the same recipe)")
     ap.add_argument("--serve-handles", type=int, default=256)
     ap.add_argument("--serve-distinct", type=int, default=256,
                     help="distinct cutout triangulations behind the handles (default: one per handle)")
@@ -128,8 +131,8 @@ def _qhull_task(task):
         pos4 = workload(key)[1]
     elif kind == "cutout":
         pos4 = W.halo_cutout(n, seed)
-    elif kind == "large":
-        pos4 = W.perturbed_lattice()
+    elif kind == "large":  # seed slot: the lattice's side
+        pos4 = W.perturbed_lattice(n_side=seed)
     else:  # "clustered": the clustered-box recipe at n particles
         pos4 = W.clustered_box(n=n, seed=seed)[0]
     t = time.perf_counter()
@@ -442,7 +445,8 @@ def plan_sections(args):
     if "serving" in sections:
         tasks += [("clustered", i, n, seed) for i, (n, seed) in enumerate(serving_cutouts(args))]
     if "large_field" in sections:
-        tasks += [("large", 0, 9_201_254, 5)]
+        side = args.large_side
+        tasks += [("large", 0, side ** 3 + round(0.3 * side ** 3), side)]
     if "plain_small" in sections and args.workload != "uniform":
         tasks += [("main", "uniform", 32768, 0)]
     return QhullPool(tasks), sections
@@ -716,7 +720,7 @@ def section_plain_small(args, sd, torch, dev, stream, flush, tri):
 
 
 def section_large_field(args, sd, torch, dev, stream, flush, tri):
-    """The large field: a 192^3 perturbed lattice plus 30% of its count in
+    """The large field: a 192^3 perturbed lattice (--large-side) plus 30% of its count in
     2,000 r^-2 clusters (float32), one 8192^2 x 4 z-projection and one 512^3
     grid (supersampling 1, the reference's column walk), mixed against FP64:
     device time, crossings, max/RMS relative error, projected mass."""
@@ -728,7 +732,8 @@ def section_large_field(args, sd, torch, dev, stream, flush, tri):
     tri.drop("large", 0)
     info = mesh.info()
     sptr = stream.cuda_stream
-    out = {"workload": "192^3 lattice (sigma 0.3 spacing) + 30% in 2000 r^-2 clusters (r 0.01), "
+    out = {"workload": f"{args.large_side}^3 lattice (sigma 0.3 spacing) + 30% in 2000 r^-2 "
+                       "clusters (r 0.01), "
                        "float32; 8192^2 x 4 map and 512^3 grid (ss 1), mixed vs FP64",
            "particles": int(len(pos4)), "tets": int(info.n_tetra), "qhull_host_s": round(t_q, 1),
            "mesh_create_s": round(t_build, 3),
