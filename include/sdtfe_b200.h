@@ -128,6 +128,10 @@ dtfe_status_t dtfe_mesh_create(const double *particle_data, int n_particles,
  * next mesh.  Work the caller enqueued on its own streams with the mesh
  * (dtfe_map_device, dtfe_grid_device, batches) must have finished first. */
 dtfe_status_t dtfe_mesh_destroy(dtfe_mesh_t mesh);
+/* Returns the current device's mesh memory that the pool keeps for reuse
+ * (up to an eighth of the device, at most 16 GB, once meshes are destroyed)
+ * to the system, for callers that need it elsewhere. */
+dtfe_status_t dtfe_trim_memory(void);
 dtfe_status_t dtfe_mesh_info(dtfe_mesh_t mesh, dtfe_mesh_info_t *info);
 dtfe_status_t dtfe_mesh_sync(dtfe_mesh_t mesh);
 

@@ -10,12 +10,12 @@ from ._lib import (AXIS_X, AXIS_Y, AXIS_Z, BATCH_GRAPH, BATCH_ZERO_MAPS, DTFE_FP
                    ERR_ADMISSION, ERR_TIMEOUT, LOCATE_PER_RAY, LOCATE_TILE, MESH_FIELD, MESH_LAZY, MESH_NO_FP64_REC, RAY_BUDGET,
                    RAY_LOC_BUDGET, RAY_MISS, RAY_NO_EXIT, RAY_OK, RAY_PERTURB_MAX, SERVE_FAIR,
                    SERVE_FIFO, Batch, DTFEError, MapParams, MapStats, Mesh, Server, lib, map_params,
-                   tetra_from_cells, triangulate)
+                   tetra_from_cells, triangulate, trim_memory)
 
 __all__ = [
     "AXIS_X", "AXIS_Y", "AXIS_Z", "BATCH_GRAPH", "BATCH_ZERO_MAPS", "DTFE_FP64", "DTFE_MIXED",
     "ERR_ADMISSION", "ERR_TIMEOUT", "LOCATE_PER_RAY", "LOCATE_TILE", "MESH_FIELD", "MESH_LAZY", "MESH_NO_FP64_REC", "RAY_BUDGET",
     "RAY_LOC_BUDGET", "RAY_MISS", "RAY_NO_EXIT", "RAY_OK", "RAY_PERTURB_MAX", "SERVE_FAIR",
     "SERVE_FIFO", "Batch", "DTFEError", "MapParams", "MapStats", "Mesh", "Server", "lib",
-    "map_params", "tetra_from_cells", "triangulate",
+    "map_params", "tetra_from_cells", "triangulate", "trim_memory",
 ]

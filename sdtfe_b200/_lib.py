@@ -172,6 +172,7 @@ def lib() -> ctypes.CDLL:
     L.dtfe_autotune.argtypes = [_vp, ctypes.POINTER(MapParams), ctypes.POINTER(_i), _vp]
     L.dtfe_set_variant.argtypes = [_vp, _i]
     L.dtfe_set_location.argtypes = [_vp, _i]
+    L.dtfe_trim_memory.argtypes = []
     L.dtfe_tetra_from_cells.argtypes = [_f64, _i32, _i32, ctypes.c_size_t, _i32]
     # batches and the serving loop
     L.dtfe_batch_create.argtypes = [ctypes.POINTER(BatchJob), _i, ctypes.c_uint, ctypes.POINTER(_vp)]
@@ -229,6 +230,11 @@ def tetra_from_cells(pos4: np.ndarray, simplices: np.ndarray, neighbors: np.ndar
     out = np.empty((len(s), 8), np.int32)
     lib().dtfe_tetra_from_cells(np.ascontiguousarray(pos4, np.float64), s, n, len(s), out)
     return out
+
+
+def trim_memory():
+    """Return the device memory the library keeps for the next mesh to the system."""
+    _check(lib().dtfe_trim_memory())
 
 
 def triangulate(pos4: np.ndarray) -> np.ndarray:

@@ -258,6 +258,12 @@ dtfe_status_t dtfe_map_device(dtfe_mesh_t h, const dtfe_map_params_t* p, double*
   return launch_map(m, p, d_map, s);
 }
 
+dtfe_status_t dtfe_trim_memory(void) {
+  SDTFE_CUDA(cudaDeviceSynchronize());  // frees still in flight on any mesh stream
+  mesh_trim_record_pool();
+  return DTFE_OK;
+}
+
 int dtfe_num_variants(void) { return num_map32_variants(); }
 
 dtfe_status_t dtfe_set_variant(dtfe_mesh_t h, int variant) {

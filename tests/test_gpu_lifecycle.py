@@ -76,3 +76,21 @@ def test_drop_in_calls_in_a_row(sd, mesh_input):
         assert (outs[0][1] > 0).all()
     finally:
         L.dtfe_set_seed(0)
+
+
+def test_trim_returns_the_pools_memory(sd, mesh_input):
+    import torch
+
+    pos4, tetra = mesh_input
+    meshes = [sd.Mesh(pos4, tetra, 1.0) for _ in range(4)]
+    for m in meshes:
+        m.map(sd.map_params(64, 1.0, 1.0, (0.5, 0.5, 0.5), 2, 0.0, 5, precision=sd.DTFE_MIXED))
+    for m in meshes:
+        m.close()
+    free_before, _ = torch.cuda.mem_get_info()
+    sd.trim_memory()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after >= free_before
+    with sd.Mesh(pos4, tetra, 1.0) as m:  # the pool refills on the next mesh
+        got, st = m.map(sd.map_params(64, 1.0, 1.0, (0.5, 0.5, 0.5), 2, 0.0, 5))
+        assert st.rays == 64 * 64 * 2 and got.sum() > 0
