@@ -289,6 +289,29 @@ def test_minimal_mesh_and_rays_outside(sd, oracle):
         assert st.status[sd.RAY_MISS] == int((rs == 1).sum()) > 0
 
 
+def test_hub_vertex_of_thousands_of_tets(sd, oracle):
+    """One vertex in most tets of a ball (the centre of points on a sphere):
+    its density is a sum over thousands of volumes, which the per-vertex sort
+    must put in the reference's order for a bit-exact result."""
+    from oracle.oracle import delaunay_tetra, to_pos4
+
+    rng = np.random.default_rng(12)
+    d = rng.normal(size=(3000, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    pts = np.vstack([[0.5, 0.5, 0.5], 0.5 + 0.3 * d * (1 + 1e-3 * rng.random((3000, 1)))])
+    pos4 = to_pos4(pts)
+    tetra = delaunay_tetra(pos4)
+    prep = oracle.prepare(pos4, tetra, 1.0)
+    with sd.Mesh(pos4, tetra, 1.0) as m:
+        adj = m.adjacency()
+        assert adj[0] > 5000  # 5,734 of the 8,016 tets
+        assert np.array_equal(adj, prep["adj"])
+        assert np.array_equal(m.density(), prep["pos"][:, 3])
+        want = oracle.map(prep, 20, 0.7, 0.7, (0.5, 0.5, 0.5), 3, 0.0, 21)
+        got, _ = m.map(sd.map_params(20, 0.7, 0.7, (0.5, 0.5, 0.5), 3, 0.0, 21))
+        assert np.array_equal(got, want)
+
+
 def test_invalid_tetra_rejected_before_any_gather(sd):
     from oracle.oracle import to_pos4
 
