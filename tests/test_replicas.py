@@ -68,3 +68,36 @@ def test_reference_arm_runs_on_rank_0_only(monkeypatch):
     args = bench.argparse.Namespace(workload="clustered", warmup=3, steps=10, cpu_seconds=15.0,
                                     gpus=2)
     assert bench.run_reference(args) is None  # returns before building anything
+
+
+def test_reference_arm_stays_off_the_library_and_matches_the_config():
+    """The reference arm on the 32k uniform workload, in a fresh interpreter:
+    it prints the same config object the GPU arm would (same tets: the numpy
+    restatement of the reference's layout equals the library's), and never
+    loads the sdtfe_b200 package or its shared library."""
+    import json
+    import subprocess
+
+    code = (
+        "import sys, json, runpy\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'uniform',\n"
+        "            '--steps', '1', '--warmup', '0', '--cpu-seconds', '1']\n"
+        "runpy.run_path('bench.py', run_name='__main__')\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'pkg': 'sdtfe_b200' in sys.modules,\n"
+        "                  'so': 'libsdtfe_b200' in maps}))\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    ref_line, probe = lines[0], lines[-1]
+    assert probe == {"pkg": False, "so": False}
+    assert ref_line["impl"] == "reference" and ref_line["value"] > 0
+
+    sys.path.insert(0, ROOT)
+    import bench
+    import sdtfe_b200 as sd
+
+    desc, pos4, spec = bench.workload("uniform")
+    tetra = sd.triangulate(pos4)
+    assert ref_line["config"] == bench.workload_config(desc, len(pos4), len(tetra), spec, 1)
